@@ -1,0 +1,136 @@
+"""ctypes binding of the C ABI in ``include/pic0buf.h`` (``lib/libpic0buf.so``).
+
+Only plain pointers and sizes cross the boundary; numpy arrays are passed by
+their data pointer.  The library must exist: there is no CPU fallback, and a
+missing or unloadable library raises ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpic0buf.so")
+
+PIC_FP64_PLAIN = 0
+PIC_FP32_MIXED = 1
+PIC_GHOSTS_REFERENCE = 0
+PIC_GHOSTS_PERIODIC = 1
+PIC_MAX_SPECIES = 8
+FIELDS = ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz", "Qx", "Qy", "Qz"]
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+
+PIC_ERR = {
+    -1: "PIC_ERR_ARG", -2: "PIC_ERR_NOMEM", -3: "PIC_ERR_STENCIL", -4: "PIC_ERR_OUTBOX", -5: "PIC_ERR_HOLES",
+    -6: "PIC_ERR_NAN", -7: "PIC_ERR_STATE", -8: "PIC_ERR_NOT_BUILT", -9: "PIC_ERR_NO_DEVICE",
+}
+
+
+class PicSpecies(C.Structure):
+    _fields_ = [("q_m", C.c_double), ("m", C.c_double), ("sort", C.c_int), ("pad_", C.c_int)]
+
+
+class PicConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+        ("tau", C.c_double),
+        ("precision", C.c_int), ("ghosts", C.c_int), ("nspecies", C.c_int), ("device", C.c_int),
+        ("species", PicSpecies * PIC_MAX_SPECIES),
+        ("capacity_slack", C.c_double), ("outbox_fraction", C.c_double),
+        ("tile", C.c_int * 3),
+        ("capacity_pad", C.c_int),
+        ("reserved", C.c_int * 7),
+    ]
+
+
+D = C.POINTER(C.c_double)
+F = C.POINTER(C.c_float)
+I32 = C.POINTER(C.c_int)
+I64 = C.POINTER(C.c_int64)
+H = C.c_void_p
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "pic_config_init": (None, [C.POINTER(PicConfig)]),
+    "pic_create": (C.c_int, [C.POINTER(PicConfig), C.POINTER(C.c_void_p)]),
+    "pic_destroy": (C.c_int, [H]),
+    "pic_load_particles": (C.c_int, [H, C.c_int, C.c_int64] + [D] * 6 + [I64]),
+    "pic_load_particles_device": (C.c_int, [H, C.c_int, C.c_int64] + [C.c_void_p] * 6 + [I64]),
+    "pic_init_species_device": (C.c_int, [H, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                          C.c_uint64]),
+    "pic_init_species_host": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                        C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64] + [D] * 6),
+    "pic_set_field": (C.c_int, [H, C.c_int, D]),
+    "pic_get_field": (C.c_int, [H, C.c_int, D]),
+    "pic_step": (C.c_int, [H, C.c_int]),
+    "pic_run": (C.c_int, [H, C.c_int, D]),
+    "pic_b_half": (C.c_int, [H]),
+    "pic_stage_fields": (C.c_int, [H]),
+    "pic_push_deposit": (C.c_int, [H]),
+    "pic_migrate": (C.c_int, [H]),
+    "pic_j_fold": (C.c_int, [H]),
+    "pic_b_complete": (C.c_int, [H]),
+    "pic_e_update": (C.c_int, [H]),
+    "pic_e_ghosts": (C.c_int, [H]),
+    "pic_get_cell_counts": (C.c_int, [H, I32]),
+    "pic_num_particles": (C.c_int64, [H, C.c_int]),
+    "pic_get_particles": (C.c_int, [H, C.c_int, C.c_int64] + [D] * 6 + [I32, I64]),
+    "pic_energy": (C.c_int, [H, D]),
+    "pic_energy_reference": (C.c_int, [H, D]),
+    "pic_charge_density": (C.c_int, [H, D]),
+    "pic_sync": (C.c_int, [H]),
+    "pic_last_status": (C.c_int, [H]),
+    "pic_last_error_string": (C.c_char_p, [H]),
+    "pic_error_string": (C.c_char_p, [C.c_int]),
+    "pic_step_counters": (C.c_int, [H, I64]),
+    "pic_step_timings": (C.c_int, [H, F]),
+    "pic_layout_info": (C.c_int, [H, I64]),
+    "pic_stream": (C.c_void_p, [H]),
+    # archAPI replacement (pic0buf_arch.h)
+    "MemoryCopy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]),
+    "MemoryAllocate": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
+    "GetDeviceMemory": (C.c_int, [C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "MemorySet": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t]),
+    "ThreadSynchronize": (C.c_int, []),
+    "DeviceSynchronize": (C.c_int, []),
+    "getLastError": (C.c_int, []),
+    "getErrorString": (C.c_char_p, [C.c_int]),
+    "SetDevice": (C.c_int, [C.c_int]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load ``libpic0buf.so`` (building nothing).  Raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"CUDA library not built: {LIB_PATH} (run python 0buf_b200/build.py)")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class PicError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        name = PIC_ERR.get(status, f"cuda error {status}" if status > 0 else str(status))
+        super().__init__(f"{where}: {name} ({detail})" if detail else f"{where}: {name}")
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(D)
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(I32)

@@ -1,0 +1,106 @@
+// Internal definitions of the B200 PIC step: geometry, device views of the
+// state, the status word and the sizes of the tile layout.
+//
+// Data layout in HBM
+//   fields   one array per component (E, H, J, Q), (Nx+2) x (Ny+2) x Pz with
+//            Pz = round_up(Nz+2, 4) so every z row starts on a 32-byte
+//            boundary (TMA rows, float4/double2 access).  The caller sees the
+//            reference layout (Pz = Nz+2) through pic_get_field/pic_set_field.
+//   particles one SoA set per species, binned by TILE: a tile is a block of
+//            tx*ty*tz interior cells; tile t owns slots
+//            [tile_start[t], tile_start[t+1]) of which the first tile_count[t]
+//            are live.  Each particle carries its int32 interior cell index
+//            ((i*Ny + l)*Nz + k); the plain form stores global FP64 positions,
+//            the mixed form FP32 in-cell offsets in [0,1).  A particle that
+//            crosses a cell boundary inside its tile only rewrites its cell
+//            index; only tile leavers move (outbox -> insert).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "pic0buf.h"
+
+namespace pic {
+
+constexpr int kMaxSpecies = PIC_MAX_SPECIES;
+constexpr int kHoleMax = 4096;          // departures per tile per species handled in-kernel
+constexpr int kPushThreads = 256;
+
+// status flag bits (DevStatus::flags)
+enum : unsigned {
+    ST_STENCIL = 1u,     // stencil index outside the staged tile (CFL)
+    ST_OUTBOX = 2u,      // outbox overflow
+    ST_HOLES = 4u,       // hole list overflow
+    ST_NAN = 8u,         // non-finite momentum
+    ST_TILE_FULL = 16u,  // arrivals did not fit their tile (kept in the outbox, rebin needed)
+    ST_BADCELL = 32u,    // a bin held a cell outside its tile, or the compaction did not pair up
+};
+
+struct DevStatus {
+    unsigned flags;
+    unsigned out_count;        // outbox entries this step
+    unsigned overflow_count;   // outbox entries that did not fit their tile
+    unsigned pad0;
+    unsigned long long moved;  // particles written to the outbox
+    unsigned long long dropped;
+    unsigned long long duplicated;
+    double kinetic;            // sum (m/q_m)(gamma-1) accumulated by the push
+    double pad1[3];
+};
+
+struct Grid {
+    int nx, ny, nz;     // interior cells
+    int NX, NY, NZ;     // nx+2, ny+2, nz+2
+    int pz;             // z pitch of device field arrays
+    int tx, ty, tz;     // cells per tile
+    int ntx, nty, ntz;  // tiles per axis
+    int ntiles;
+    double lx, ly, lz, hx, hy, hz, tau;
+    __host__ __device__ size_t nodes_pitched() const { return (size_t)NX * NY * pz; }
+    __host__ __device__ size_t nodes_ref() const { return (size_t)NX * NY * NZ; }
+    __host__ __device__ size_t node(int i, int l, int k) const { return ((size_t)i * NY + l) * pz + k; }
+    __host__ __device__ int ncells() const { return nx * ny * nz; }
+    __host__ __device__ int cell_of(int i, int l, int k) const { return (i * ny + l) * nz + k; }
+    __host__ __device__ int tile_of_cell(int i, int l, int k) const {
+        return ((i / tx) * nty + (l / ty)) * ntz + (k / tz);
+    }
+};
+
+struct SpeciesView {
+    // plain form
+    double *x, *y, *z, *px, *py, *pz;
+    // mixed form
+    float *ox, *oy, *oz, *fx, *fy, *fz;
+    int *cell;
+    int *tile_start;  // ntiles + 1
+    int *tile_count;  // ntiles
+    double q_m, m;
+};
+
+// one migrating particle (plain form): 56 bytes
+struct OutPlain {
+    double x, y, z, px, py, pz;
+    int cell, species;
+};
+// one migrating particle (mixed form): 32 bytes
+struct OutMixed {
+    float ox, oy, oz, px, py, pz;
+    int cell, species;
+};
+
+struct StepParams {
+    Grid g;
+    int nsp;
+    int mixed;
+    SpeciesView sp[kMaxSpecies];
+    // plain: double fields; mixed: float E/H, double J
+    const void *E[3];
+    const void *H[3];
+    double *J[3];
+    void *outbox;
+    unsigned out_cap;
+    DevStatus *st;
+};
+
+
+}  // namespace pic

@@ -1,0 +1,283 @@
+"""Host-side mirror of the reference's step driver, over the C ABI.
+
+``PicSimulation`` is a thin owner of one ``pic_handle``.  ``Plasma`` keeps the
+reference's host surface (class Plasma, gpu_plasma.h:97-2355): the same
+constructor arguments as ``main.cu:14``, ``Initialize`` / ``Compute`` /
+``Step`` and the sub-steps of ``Step`` with their control-point ids, so that a
+user of the reference finds the same names.  All arithmetic runs in the CUDA
+library; this module only moves arguments and arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import PicConfig, PicError, dptr, iptr
+from .configs import SPECIES_BEAM_PLASMA, charge_weight
+
+
+class PicSimulation:
+    """One PIC state on one GPU (``pic_create`` .. ``pic_destroy``)."""
+
+    def __init__(self, cells: Sequence[int], lengths: Sequence[float], tau: float,
+                 species: Sequence[tuple], precision: str = "fp64", ghosts: str = "reference",
+                 device: int = 0, tile: Sequence[int] | None = None, capacity_slack: float = 0.25,
+                 outbox_fraction: float = 0.04, capacity_pad: int = -1):
+        self.lib = _capi.load()
+        cfg = PicConfig()
+        self.lib.pic_config_init(C.byref(cfg))
+        cfg.nx, cfg.ny, cfg.nz = (int(c) for c in cells)
+        cfg.lx, cfg.ly, cfg.lz = (float(v) for v in lengths)
+        cfg.tau = float(tau)
+        cfg.precision = {"fp64": _capi.PIC_FP64_PLAIN, "fp32": _capi.PIC_FP32_MIXED}[precision]
+        cfg.ghosts = {"reference": _capi.PIC_GHOSTS_REFERENCE, "periodic": _capi.PIC_GHOSTS_PERIODIC}[ghosts]
+        cfg.nspecies = len(species)
+        for i, (q_m, m, sort) in enumerate(species):
+            cfg.species[i].q_m = q_m
+            cfg.species[i].m = m
+            cfg.species[i].sort = sort
+        cfg.device = device
+        cfg.capacity_slack = capacity_slack
+        cfg.outbox_fraction = outbox_fraction
+        cfg.capacity_pad = capacity_pad
+        if tile is not None:
+            for a in range(3):
+                cfg.tile[a] = int(tile[a])
+        self.cfg = cfg
+        self.precision = precision
+        self.cells = tuple(int(c) for c in cells)
+        self.shape = tuple(c + 2 for c in self.cells)
+        self.nspecies = len(species)
+        h = C.c_void_p()
+        rc = self.lib.pic_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise PicError(rc, "pic_create")
+        self.h = h
+
+    # ------------------------------------------------------------- helpers
+    def _ck(self, rc: int, where: str):
+        if rc != 0:
+            detail = self.lib.pic_last_error_string(self.h).decode(errors="replace") if self.h else ""
+            raise PicError(rc, where, detail)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pic_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ----------------------------------------------------------- particles
+    def load_particles(self, species: int, x, y, z, px, py, pz) -> int:
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, px, py, pz)]
+        n = arrs[0].size
+        ins = C.c_int64(0)
+        self._ck(self.lib.pic_load_particles(self.h, species, n, *[dptr(a) for a in arrs], C.byref(ins)),
+                 "pic_load_particles")
+        return ins.value
+
+    def init_species(self, species: int, ppc: int, drift=(0.0, 0.0, 0.0), vth: float = 0.0, seed: int = 0):
+        self._ck(self.lib.pic_init_species_device(self.h, species, ppc, *[float(d) for d in drift], float(vth),
+                                                  int(seed)), "pic_init_species_device")
+
+    def num_particles(self, species: int = -1) -> int:
+        n = self.lib.pic_num_particles(self.h, species)
+        if n < 0:
+            self._ck(int(n), "pic_num_particles")
+        return int(n)
+
+    def particles(self, species: int) -> dict:
+        n = self.num_particles(species)
+        out = {k: np.zeros(max(n, 1)) for k in ("x", "y", "z", "px", "py", "pz")}
+        cell = np.zeros(max(n, 1), np.int32)
+        got = C.c_int64(0)
+        self._ck(self.lib.pic_get_particles(self.h, species, max(n, 1), *[dptr(out[k]) for k in
+                                            ("x", "y", "z", "px", "py", "pz")], iptr(cell), C.byref(got)),
+                 "pic_get_particles")
+        m = got.value
+        res = {k: v[:m] for k, v in out.items()}
+        res["cell"] = cell[:m]
+        return res
+
+    def cell_counts(self) -> np.ndarray:
+        c = np.zeros(int(np.prod(self.shape)), np.int32)
+        self._ck(self.lib.pic_get_cell_counts(self.h, iptr(c)), "pic_get_cell_counts")
+        return c
+
+    # -------------------------------------------------------------- fields
+    def get_field(self, name: str) -> np.ndarray:
+        a = np.zeros(int(np.prod(self.shape)))
+        self._ck(self.lib.pic_get_field(self.h, _capi.FIELD_ID[name], dptr(a)), f"pic_get_field({name})")
+        return a
+
+    def set_field(self, name: str, values: np.ndarray):
+        a = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        assert a.size == int(np.prod(self.shape))
+        self._ck(self.lib.pic_set_field(self.h, _capi.FIELD_ID[name], dptr(a)), f"pic_set_field({name})")
+
+    def fields(self, names=_capi.FIELDS) -> dict:
+        return {n: self.get_field(n) for n in names}
+
+    # --------------------------------------------------------------- steps
+    def step(self, nt: int = 0):
+        self._ck(self.lib.pic_step(self.h, nt), "pic_step")
+
+    def run(self, nsteps: int, energies: bool = False):
+        if energies:
+            e = np.zeros((nsteps, 4))
+            self._ck(self.lib.pic_run(self.h, nsteps, dptr(e)), "pic_run")
+            return e
+        self._ck(self.lib.pic_run(self.h, nsteps, None), "pic_run")
+        return None
+
+    def substep(self, name: str):
+        self._ck(getattr(self.lib, "pic_" + name)(self.h), "pic_" + name)
+
+    def sync(self):
+        self._ck(self.lib.pic_sync(self.h), "pic_sync")
+
+    # --------------------------------------------------------- diagnostics
+    def energy(self) -> np.ndarray:
+        e = np.zeros(4)
+        self._ck(self.lib.pic_energy(self.h, dptr(e)), "pic_energy")
+        return e
+
+    def energy_reference(self) -> float:
+        e = np.zeros(1)
+        self._ck(self.lib.pic_energy_reference(self.h, dptr(e)), "pic_energy_reference")
+        return float(e[0])
+
+    def counters(self) -> np.ndarray:
+        c = np.zeros(4, np.int64)
+        self.lib.pic_step_counters(self.h, c.ctypes.data_as(_capi.I64))
+        return c
+
+    def timings(self) -> np.ndarray:
+        t = np.zeros(4, np.float32)
+        self.lib.pic_step_timings(self.h, t.ctypes.data_as(_capi.F))
+        return t
+
+    def layout(self) -> dict:
+        v = np.zeros(4, np.int64)
+        self._ck(self.lib.pic_layout_info(self.h, v.ctypes.data_as(_capi.I64)), "pic_layout_info")
+        return dict(tiles=int(v[0]), slots=int(v[1]), bytes_per_particle=int(v[2]), nodes=int(v[3]))
+
+
+def host_species(cells, lengths, species_index: int, ppc: int, drift=(0.0, 0.0, 0.0), vth: float = 0.0,
+                 seed: int = 0):
+    """The seeded generator on the host (``pic_init_species_host``): x, y, z, px, py, pz arrays."""
+    lib = _capi.load()
+    n = int(np.prod(cells)) * ppc
+    arrs = [np.zeros(n) for _ in range(6)]
+    rc = lib.pic_init_species_host(int(cells[0]), int(cells[1]), int(cells[2]), *[float(v) for v in lengths],
+                                   species_index, ppc, *[float(d) for d in drift], float(vth), int(seed),
+                                   *[dptr(a) for a in arrs])
+    if rc != 0:
+        raise PicError(rc, "pic_init_species_host")
+    return arrs
+
+
+class Plasma:
+    """Mirror of the reference's ``class Plasma`` (gpu_plasma.h:97).
+
+    ``Plasma(Nx, Ny, Nz, Lx, Ly, Lz, ni, n_per_cell, ion_q_m, tau)`` takes the
+    arguments of the reference constructor (gpu_plasma.h:1574-1589, called as
+    in main.cu:14).  ``Initialize`` loads the beam-plasma species of the
+    benchmark configurations (ions of q/m = ion_q_m and density 1.01*ni,
+    electrons of density ni, beam of density 0.01*ni) with ``n_per_cell``
+    particles per cell per species from a seeded generator, replacing the
+    reference's hard-coded loader (maxwell.cu:676-757).
+    """
+
+    TOTAL_STEPS = 5  # run_control.h:10
+
+    def __init__(self, Nx, Ny, Nz, Lx, Ly, Lz, ni, n_per_cell, ion_q_m, tau, precision="fp64",
+                 ghosts="reference", device=0, seed=0, species=None):
+        self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
+        self.Lx, self.Ly, self.Lz = Lx, Ly, Lz
+        self.ni, self.n_per_cell, self.ion_q_m, self.tau = ni, n_per_cell, ion_q_m, tau
+        self.seed = seed
+        if species is None:
+            species = [dict(s) for s in SPECIES_BEAM_PLASMA]
+            species[0]["q_m"] = ion_q_m
+            for s in species:
+                s["density"] = s["density"] * ni
+        self.species = species
+        table = [(s["q_m"], charge_weight(s["q_m"], s["density"], n_per_cell), s["sort"]) for s in species]
+        self.sim = PicSimulation((Nx, Ny, Nz), (Lx, Ly, Lz), tau, table, precision=precision, ghosts=ghosts,
+                                 device=device)
+        self.energy_history = []
+        self.control_points = []
+
+    # Initialize, init.cu:141-152
+    def Initialize(self, host_generator: bool = False):
+        for i, s in enumerate(self.species):
+            if host_generator:
+                arrs = host_species((self.Nx, self.Ny, self.Nz), (self.Lx, self.Ly, self.Lz), i, self.n_per_cell,
+                                    s["drift"], s["vth"], self.seed)
+                self.sim.load_particles(i, *arrs)
+            else:
+                self.sim.init_species(i, self.n_per_cell, s["drift"], s["vth"], self.seed)
+
+    # ComputeField_FirstHalfStep, gpu_plasma.h:367-397 (control point 50)
+    def ComputeField_FirstHalfStep(self, nt):
+        self.sim.substep("b_half")
+        self.checkControlPoint(50, nt)
+        self.sim.substep("stage_fields")
+
+    # PushParticles, gpu_plasma.h:554-570 (control point 270)
+    def PushParticles(self, nt):
+        self.sim.substep("push_deposit")
+        self.sim.substep("migrate")
+        self.checkControlPoint(270, nt)
+
+    # ComputeField_SecondHalfStep, gpu_plasma.h:399-414 (control points 275, 400, 500, 550, 600)
+    def ComputeField_SecondHalfStep(self, nt):
+        self.checkControlPoint(275, nt)
+        self.sim.substep("j_fold")
+        self.checkControlPoint(400, nt)
+        self.sim.substep("b_complete")
+        self.checkControlPoint(500, nt)
+        self.sim.substep("e_update")
+        self.checkControlPoint(550, nt)
+        self.sim.substep("e_ghosts")
+        self.checkControlPoint(600, nt)
+
+    # Step, gpu_plasma.h:605-620 (the MPI sum of J is not part of the one-GPU step)
+    def Step(self, nt):
+        self.ComputeField_FirstHalfStep(nt)
+        self.PushParticles(nt)
+        self.ComputeField_SecondHalfStep(nt)
+        self.Diagnose(nt)
+
+    # Compute, gpu_plasma.h:2329-2352
+    def Compute(self, total_steps=None):
+        for nt in range(1, (total_steps or self.TOTAL_STEPS) + 1):
+            self.Step(nt)
+
+    # getElectricEnergy / Diagnose, gpu_plasma.h:621-686
+    def getElectricEnergy(self) -> float:
+        return self.sim.energy_reference()
+
+    def Diagnose(self, nt):
+        self.energy_history.append((nt, self.getElectricEnergy()))
+
+    # checkControlPoint, gpu_plasma.h:1170-1284: a hook, see compare.ControlPointChecker
+    checker = None
+
+    def checkControlPoint(self, num, nt):
+        if self.checker is not None:
+            self.control_points.append(self.checker(self, num, nt))

@@ -1,0 +1,192 @@
+/*
+ * pic0buf.h -- C ABI of the B200 (sm_100a) 3D electromagnetic PIC time step.
+ *
+ * This header is the drop-in boundary for the 0buf PIC step.  It replaces
+ *   - the reference's arch layer archAPI.h:1-127 (see pic0buf_arch.h), and
+ *   - the ~20 cudaLaunchKernel sites of the reference step driver
+ *     (class Plasma, gpu_plasma.h:97-2355), which become the pic_* calls below.
+ *
+ * Conventions kept from the reference:
+ *   - every call returns an int status; 0 is success (archAPI.cu:53 returns the
+ *     CUDA error code, which is what positive values here are); negative values
+ *     are PIC errors (PIC_ERR_*).  No call exits the process.
+ *   - field arrays cross the boundary in the reference layout: FP64,
+ *     (Nx+2)(Ny+2)(Nz+2) nodes, index i*(Ny+2)*(Nz+2) + l*(Nz+2) + k
+ *     (Cell::getGlobalCellNumber, cell.h:796-801).
+ *   - cell numbers reported to the caller use the same (Nx+2)(Ny+2)(Nz+2)
+ *     numbering; particles only live in the interior cells.
+ *   - one host thread per handle; each handle owns one CUDA stream and all
+ *     calls on a handle are ordered on it.
+ *
+ * Plain pointers and sizes only; no C++ or torch types.
+ */
+#ifndef PIC0BUF_H
+#define PIC0BUF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIC0BUF_ABI_VERSION 1
+
+/* precision forms */
+#define PIC_FP64_PLAIN 0 /* FP64, reference arithmetic (parity form) */
+#define PIC_FP32_MIXED 1 /* FP32 push/deposit/Yee, int32 cell + FP32 offsets, FP64 global J */
+
+/* E ghost refresh (gpu_plasma.h:432-452 skips the y pass for Ex and Ez) */
+#define PIC_GHOSTS_REFERENCE 0
+#define PIC_GHOSTS_PERIODIC 1
+
+#define PIC_MAX_SPECIES 8
+
+/* field ids for pic_get_field / pic_set_field (Plasma members, gpu_plasma.h:705-707) */
+enum pic_field_id {
+    PIC_EX = 0, PIC_EY, PIC_EZ,
+    PIC_HX, PIC_HY, PIC_HZ,
+    PIC_JX, PIC_JY, PIC_JZ,
+    PIC_QX, PIC_QY, PIC_QZ, /* half-step magnetic increment (emh1_Element, kernels.cu:1052-1073) */
+    PIC_FIELD_COUNT
+};
+
+/* errors (negative) */
+#define PIC_OK 0
+#define PIC_ERR_ARG (-1)            /* bad argument or config */
+#define PIC_ERR_NOMEM (-2)          /* device or host allocation failed */
+#define PIC_ERR_STENCIL (-3)        /* a particle moved more than half a cell (CFL), stencil left the tile */
+#define PIC_ERR_OUTBOX (-4)         /* migration outbox overflowed */
+#define PIC_ERR_HOLES (-5)          /* more departures from one tile than the compaction list holds */
+#define PIC_ERR_NAN (-6)            /* non-finite momentum after the push */
+#define PIC_ERR_STATE (-7)          /* call not valid in the current state */
+#define PIC_ERR_NOT_BUILT (-8)      /* feature not available in this build */
+#define PIC_ERR_NO_DEVICE (-9)      /* no CUDA device */
+#define PIC_ERR_TOO_MANY (-513131313) /* TOO_MANY_PARTICLES, cell.h:27 (never raised: no per-cell cap) */
+
+typedef struct pic_species {
+    double q_m;  /* charge to mass ratio (Particle::q_m, particle.h:43) */
+    double m;    /* signed charge weight of one macro-particle (Particle::m, particle.h:43) */
+    int sort;    /* particle_sorts id, particle_types.h:11 (0 ion, 1 plasma electron, 2 beam) */
+    int pad_;
+} pic_species;
+
+typedef struct pic_config {
+    int nx, ny, nz;          /* interior cells per axis (Plasma::Nx.., gpu_plasma.h:691); each >= 3 */
+    double lx, ly, lz;       /* box lengths; h = L/N (Cell ctor, cell.h:731-737) */
+    double tau;              /* time step (Plasma::tau) */
+    int precision;           /* PIC_FP64_PLAIN or PIC_FP32_MIXED */
+    int ghosts;              /* PIC_GHOSTS_REFERENCE or PIC_GHOSTS_PERIODIC */
+    int nspecies;            /* 1..PIC_MAX_SPECIES */
+    int device;              /* CUDA device ordinal */
+    pic_species species[PIC_MAX_SPECIES];
+    double capacity_slack;   /* particle slots per tile = count * (1 + slack) + pad; 0 -> 0.25 */
+    double outbox_fraction;  /* outbox slots = fraction * total capacity + 65536; 0 -> 0.04 */
+    int tile[3];             /* cells per tile (x, y, z); 0 -> automatic. tile[2] % 4 == 0 */
+    int capacity_pad;        /* extra slots per tile; negative -> 64 */
+    int reserved[7];
+} pic_config;
+
+typedef struct pic_handle pic_handle;
+
+/* Fill a config with defaults (precision FP64 plain, reference ghosts, device 0). */
+void pic_config_init(pic_config *cfg);
+
+int pic_create(const pic_config *cfg, pic_handle **out);
+int pic_destroy(pic_handle *h);
+
+/* Loads (replaces) one species from HOST arrays of global positions and
+ * momenta (p = gamma*v, c = 1), in the reference's initial placement:
+ * getPointCell + Cell::Insert (init.cu:558-592, cell.h:585-598, 1754-1768).
+ * Particles that no cell accepts are dropped; *inserted (may be NULL) gets the
+ * number kept. */
+int pic_load_particles(pic_handle *h, int species, int64_t n, const double *x, const double *y,
+                       const double *z, const double *px, const double *py, const double *pz,
+                       int64_t *inserted);
+/* Same from DEVICE arrays. */
+int pic_load_particles_device(pic_handle *h, int species, int64_t n, const double *x, const double *y,
+                              const double *z, const double *px, const double *py, const double *pz,
+                              int64_t *inserted);
+
+/* Seeded uniform-in-cell / Maxwellian species generated on the device:
+ * ppc particles per interior cell at uniform in-cell offsets, momenta
+ * drift + vth * N(0,1) per axis.  Keyed by (seed, species, cell, slot). */
+int pic_init_species_device(pic_handle *h, int species, int ppc, double drift_x, double drift_y,
+                            double drift_z, double vth, uint64_t seed);
+/* The same generator on the host (writes n = Nx*Ny*Nz*ppc particles). */
+int pic_init_species_host(int nx, int ny, int nz, double lx, double ly, double lz, int species_index, int ppc,
+                          double drift_x, double drift_y, double drift_z, double vth, uint64_t seed,
+                          double *x, double *y, double *z, double *px, double *py, double *pz);
+
+/* Fields in the reference layout, FP64 host arrays of (Nx+2)(Ny+2)(Nz+2). */
+int pic_set_field(pic_handle *h, int field, const double *host);
+int pic_get_field(pic_handle *h, int field, double *host);
+
+/* One full time step, Plasma::Step (gpu_plasma.h:605-620) without the MPI sum. */
+int pic_step(pic_handle *h, int nt);
+/* n steps back to back; if energies != NULL it receives 4 doubles per step
+ * (pic_energy after each step). */
+int pic_run(pic_handle *h, int nsteps, double *energies);
+
+/* Sub-steps, in Plasma::Step order, so the control points map 1:1:
+ *   pic_b_half        MagneticStageOne            gpu_plasma.h:524-538   (cp 50 after)
+ *   pic_stage_fields  AssignCellsToArraysGPU      gpu_plasma.h:1006-1036 (no-op: staged in-kernel)
+ *   pic_push_deposit  SetCurrentsToZero + Push + WriteCurrentsFromCellsToArrays
+ *                                                 gpu_plasma.h:2058-2090
+ *   pic_migrate       reorder_particles           gpu_plasma.h:2035-2046 (cp 270 after)
+ *   pic_j_fold        SetPeriodicCurrents         gpu_plasma.h:980-993   (cp 275 before, 400 after)
+ *   pic_b_complete    MagneticFieldStageTwo       gpu_plasma.h:540-551   (cp 500 after)
+ *   pic_e_update      ElectricFieldEvaluate traces gpu_plasma.h:455-483  (cp 550 after)
+ *   pic_e_ghosts      ElectricFieldComponentEvaluatePeriodic x3 gpu_plasma.h:486-507 (cp 600 after)
+ */
+int pic_b_half(pic_handle *h);
+int pic_stage_fields(pic_handle *h);
+int pic_push_deposit(pic_handle *h);
+int pic_migrate(pic_handle *h);
+int pic_j_fold(pic_handle *h);
+int pic_b_complete(pic_handle *h);
+int pic_e_update(pic_handle *h);
+int pic_e_ghosts(pic_handle *h);
+
+/* Particle counts per cell over all species, reference numbering,
+ * (Nx+2)(Ny+2)(Nz+2) ints (ghost cells 0). */
+int pic_get_cell_counts(pic_handle *h, int *counts);
+int64_t pic_num_particles(pic_handle *h, int species); /* species < 0: all; negative on error */
+/* Exports one species to host arrays (capacity cap); positions are global
+ * FP64 (the mixed form converts cell + offset).  cell gets the reference cell
+ * number.  *n receives the count.  Order is the device bin order. */
+int pic_get_particles(pic_handle *h, int species, int64_t cap, double *x, double *y, double *z,
+                      double *px, double *py, double *pz, int *cell, int64_t *n);
+
+/* FP64 diagnostics: out[0] = 1/2 sum E^2, out[1] = 1/2 sum H^2 over nodes
+ * 1..N of every axis, out[2] = kinetic sum (m/q_m)(gamma-1), out[3] = total.
+ * The reference has only sum E^2 over all nodes (GPU_getCellEnergy,
+ * wrap_kernel.cu:14-36), which pic_energy_reference returns. */
+int pic_energy(pic_handle *h, double *out4);
+int pic_energy_reference(pic_handle *h, double *out);
+/* Charge-conservation residual: max |div E - div E(t0) + (rho - rho(t0))|
+ * style check -- see pic_charge_residual in the implementation notes. */
+int pic_charge_density(pic_handle *h, double *rho_host);
+
+/* Status and errors. */
+int pic_sync(pic_handle *h);
+int pic_last_status(pic_handle *h);
+const char *pic_last_error_string(pic_handle *h);
+const char *pic_error_string(int status);
+/* Per-step counters of the last step: [0] particles moved to another tile,
+ * [1] particles no cell accepted (dropped), [2] particles two or more cells
+ * accepted (duplicated), [3] tile slots in use (max over tiles, percent). */
+int pic_step_counters(pic_handle *h, int64_t *out4);
+/* Timings of the last pic_step in milliseconds (CUDA events on the handle's
+ * stream): [0] b_half [1] push_deposit [2] migrate [3] fields second half. */
+int pic_step_timings(pic_handle *h, float *out4);
+/* Internal sizes for the roofline: [0] tiles [1] total particle slots
+ * [2] bytes per particle (28 mixed / 52 plain) [3] field nodes. */
+int pic_layout_info(pic_handle *h, int64_t *out4);
+/* The CUDA stream of the handle, as void* (cudaStream_t). */
+void *pic_stream(pic_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIC0BUF_H */

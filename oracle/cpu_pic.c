@@ -667,8 +667,8 @@ int op_energies(void *h, double *out) {
         op_cell *c = &s->cells[ci];
         for (int j = 0; j < c->n; j++) {
             op_particle *p = &c->p[j];
-            double g = sqrt(1.0 + p->pu * p->pu + p->pv * p->pv + p->pw * p->pw);
-            wk += (p->m / p->q_m) * (g - 1.0);
+            double p2 = p->pu * p->pu + p->pv * p->pv + p->pw * p->pw;
+            wk += (p->m / p->q_m) * (p2 / (sqrt(1.0 + p2) + 1.0)); /* gamma - 1 without cancellation */
         }
     }
     out[0] = 0.5 * we;

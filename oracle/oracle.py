@@ -1,0 +1,194 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY.
+
+ctypes wrappers of the two CPU implementations of the 0buf PIC step that the
+tests use as checkers (never imported by the product package):
+
+- ``OracleSim``: the C restatement ``oracle/cpu_pic.c`` (lib/libpicoracle.so)
+- ``RefSim``: the reference's own functions replayed on the host
+  (``oracle/ref_driver.cu`` -> _ref/libref0buf.so, built only where the
+  reference sources exist)
+
+Both expose the same methods, sub-step ids and export layout.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "lib", "libpicoracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref0buf.so")
+
+SUBSTEPS = ["b_half", "stage", "zero_j", "push", "deposit", "write_j", "migrate", "j_fold", "b_complete",
+            "e_update", "e_ghosts"]
+FIELDS = ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz", "Qx", "Qy", "Qz"]
+
+D = C.POINTER(C.c_double)
+I = C.POINTER(C.c_int)
+
+
+def build_oracle() -> str:
+    """Compile cpu_pic.c (make) if the library is missing or stale."""
+    src = os.path.join(HERE, "cpu_pic.c")
+    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    return ORACLE_LIB
+
+
+def _bind(lib, p):
+    def f(name, res, args):
+        fn = getattr(lib, p + name)
+        fn.restype = res
+        fn.argtypes = args
+    f("create", C.c_void_p, [C.c_int] * 3 + [C.c_double] * 4)
+    f("destroy", None, [C.c_void_p])
+    f("add_particles", C.c_long, [C.c_void_p, C.c_int, C.c_long] + [D] * 6 + [C.c_double] * 2)
+    f("set_field", C.c_int, [C.c_void_p, C.c_int, D])
+    f("get_field", C.c_int, [C.c_void_p, C.c_int, D])
+    f("substep", C.c_int, [C.c_void_p, C.c_int])
+    f("step", C.c_int, [C.c_void_p])
+    f("energy", C.c_double, [C.c_void_p])
+    f("num_particles", C.c_long, [C.c_void_p])
+    f("get_particles", C.c_long, [C.c_void_p, D, I, I, I])
+    f("get_cell_counts", C.c_int, [C.c_void_p, I])
+
+
+class _Sim:
+    prefix = ""
+    libpath = ""
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(cls.libpath):
+                raise FileNotFoundError(cls.libpath)
+            lib = C.CDLL(cls.libpath)
+            _bind(lib, cls.prefix)
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, cells, lengths, tau, threads: int = 1):
+        self.L = self.lib()
+        self.cells = tuple(int(c) for c in cells)
+        self.shape = tuple(c + 2 for c in self.cells)
+        self.nodes = int(np.prod(self.shape))
+        self.h = self._f("create")(*self.cells, *[float(v) for v in lengths], float(tau))
+        if not self.h:
+            raise ValueError("bad grid")
+        self.set_threads(threads)
+
+    def _f(self, name):
+        return getattr(self.L, self.prefix + name)
+
+    def set_threads(self, n):
+        pass
+
+    def close(self):
+        if self.h:
+            self._f("destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_particles(self, sort, x, y, z, px, py, pz, m, q_m) -> int:
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, px, py, pz)]
+        return int(self._f("add_particles")(self.h, sort, arrs[0].size, *[a.ctypes.data_as(D) for a in arrs],
+                                            float(m), float(q_m)))
+
+    def set_field(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+        assert a.size == self.nodes
+        assert self._f("set_field")(self.h, FIELDS.index(name), a.ctypes.data_as(D)) == 0
+
+    def get_field(self, name):
+        a = np.zeros(self.nodes)
+        assert self._f("get_field")(self.h, FIELDS.index(name), a.ctypes.data_as(D)) == 0
+        return a
+
+    def fields(self, names=FIELDS):
+        return {n: self.get_field(n) for n in names}
+
+    def substep(self, name) -> int:
+        return int(self._f("substep")(self.h, SUBSTEPS.index(name)))
+
+    def step(self) -> int:
+        return int(self._f("step")(self.h))
+
+    def energy_reference(self) -> float:
+        return float(self._f("energy")(self.h))
+
+    def num_particles(self) -> int:
+        return int(self._f("num_particles")(self.h))
+
+    def cell_counts(self):
+        c = np.zeros(self.nodes, np.int32)
+        self._f("get_cell_counts")(self.h, c.ctypes.data_as(I))
+        return c
+
+    def particles(self):
+        """All particles in cell order then list order: dict of x y z px py pz m q_m x1 y1 z1, cell, sort, dir."""
+        n = self.num_particles()
+        P = np.zeros((max(n, 1), 11))
+        cell = np.zeros(max(n, 1), np.int32)
+        sort = np.zeros(max(n, 1), np.int32)
+        d = np.zeros(max(n, 1), np.int32)
+        self._f("get_particles")(self.h, P.ctypes.data_as(D), cell.ctypes.data_as(I), sort.ctypes.data_as(I),
+                                 d.ctypes.data_as(I))
+        keys = ["x", "y", "z", "px", "py", "pz", "m", "q_m", "x1", "y1", "z1"]
+        out = {k: P[:n, i].copy() for i, k in enumerate(keys)}
+        out.update(cell=cell[:n].copy(), sort=sort[:n].copy(), dir=d[:n].copy())
+        return out
+
+
+class OracleSim(_Sim):
+    """The C restatement (oracle/cpu_pic.c)."""
+    prefix = "op_"
+    libpath = ORACLE_LIB
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            build_oracle()
+            lib = super().lib()
+            lib.op_set_threads.argtypes = [C.c_void_p, C.c_int]
+            lib.op_energies.argtypes = [C.c_void_p, D]
+            lib.op_energies.restype = C.c_int
+            lib.op_status.argtypes = [C.c_void_p]
+            lib.op_status.restype = C.c_int
+        return cls._lib
+
+    def set_threads(self, n):
+        self.L.op_set_threads(self.h, int(n))
+
+    def energies(self):
+        e = np.zeros(4)
+        self.L.op_energies(self.h, e.ctypes.data_as(D))
+        return e
+
+
+class RefSim(_Sim):
+    """The reference's own functions replayed on the host (oracle/ref_driver.cu)."""
+    prefix = "ref_"
+    libpath = REF_LIB
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = super().lib()
+            lib.ref_set_threads.argtypes = [C.c_int]
+        return cls._lib
+
+    def set_threads(self, n):
+        self.L.ref_set_threads(int(n))
+
+    @classmethod
+    def available(cls) -> bool:
+        return os.path.exists(cls.libpath)

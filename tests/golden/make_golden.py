@@ -1,0 +1,118 @@
+"""Generates the golden fixtures of the 0buf PIC step from the REFERENCE'S OWN
+functions (cell.h / particle.h / kernels.cu compiled for the host by
+oracle/build_ref.sh and replayed by oracle/ref_driver.cu).
+
+Run in a container that has the reference sources:
+    python tests/golden/make_golden.py
+Writes tests/golden/ref_small.npz and tests/golden/ref_c0.npz.  The inputs come
+from the product's host generator (pic_init_species_host, seeded); they are
+stored in the fixture (small case) or pinned by a digest (c0 case) so the
+fixtures stand alone.
+"""
+from __future__ import annotations
+
+import hashlib
+import importlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+pkg = importlib.import_module("0buf_b200")
+from oracle import RefSim, FIELDS, SUBSTEPS  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def digest(a: np.ndarray) -> str:
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.float64:
+        a = np.where(a == 0.0, 0.0, a)  # -0.0 and +0.0 hash alike
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def species_inputs(cells, lengths, ppc, seed):
+    out = []
+    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
+        arrs = pkg.host_species(cells, lengths, i, ppc, s["drift"], s["vth"], seed)
+        m = pkg.configs.charge_weight(s["q_m"], s["density"], ppc)
+        out.append((s["sort"], arrs, m, s["q_m"]))
+    return out
+
+
+def particle_table(p):
+    return np.stack([p["cell"].astype(np.float64), p["sort"].astype(np.float64), p["x"], p["y"], p["z"], p["px"],
+                     p["py"], p["pz"]], axis=1)
+
+
+def make_small():
+    cells, h, tau, ppc, seed, steps = (8, 4, 4), 0.1, 0.02, 3, 7, 4
+    # arrays each sub-step changes (snapshotted after that sub-step of step 1)
+    changed = dict(b_half=("Hx", "Hy", "Hz", "Qx", "Qy", "Qz"), write_j=("Jx", "Jy", "Jz"),
+                   j_fold=("Jx", "Jy", "Jz"), b_complete=("Hx", "Hy", "Hz"), e_update=("Ex", "Ey", "Ez"),
+                   e_ghosts=("Ex", "Ey", "Ez"))
+    lengths = tuple(c * h for c in cells)
+    sim = RefSim(cells, lengths, tau)
+    inputs = species_inputs(cells, lengths, ppc, seed)
+    rec = dict(cells=np.array(cells), h=h, tau=tau, ppc=ppc, seed=seed, steps=steps)
+    for sort, arrs, m, q_m in inputs:
+        sim.add_particles(sort, *arrs, m, q_m)
+        for k, a in zip(("x", "y", "z", "px", "py", "pz"), arrs):
+            rec[f"in_s{sort}_{k}"] = a
+        rec[f"in_s{sort}_m"] = m
+        rec[f"in_s{sort}_q_m"] = q_m
+    rng = np.random.default_rng(seed)
+    for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        a = rng.normal(0.0, 1e-3, sim.nodes)
+        sim.set_field(f, a)
+        rec[f"in_{f}"] = a
+    for st in range(1, steps + 1):
+        for sub in SUBSTEPS:
+            rc = sim.substep(sub)
+            assert rc == 0, (sub, rc)
+            if st == 1 and sub in changed:
+                for f in changed[sub]:
+                    rec[f"sub_{sub}_{f}"] = sim.get_field(f)
+            if st == 1 and sub == "migrate":
+                rec["sub_migrate_particles"] = particle_table(sim.particles())
+        for f in FIELDS:
+            rec[f"step{st}_{f}"] = sim.get_field(f)
+        rec[f"step{st}_counts"] = sim.cell_counts()
+        rec[f"step{st}_energy"] = sim.energy_reference()
+        if st in (1, steps):
+            rec[f"step{st}_particles"] = particle_table(sim.particles())
+    np.savez_compressed(os.path.join(OUT, "ref_small.npz"), **rec)
+
+
+def make_c0(steps=10):
+    cfg = pkg.configs.CONFIGS["c0"]
+    cells, h, tau, ppc, seed = cfg["cells"], cfg["h"], cfg["tau"], cfg["ppc"], 0
+    lengths = tuple(c * h for c in cells)
+    sim = RefSim(cells, lengths, tau, threads=os.cpu_count() or 1)
+    inputs = species_inputs(cells, lengths, ppc, seed)
+    rec = dict(cells=np.array(cells), h=h, tau=tau, ppc=ppc, seed=seed, steps=steps)
+    rec["inputs_digest"] = digest(np.concatenate([a for _, arrs, _, _ in inputs for a in arrs]))
+    for sort, arrs, m, q_m in inputs:
+        sim.add_particles(sort, *arrs, m, q_m)
+    for st in range(1, steps + 1):
+        assert sim.step() == 0
+        for f in FIELDS:
+            rec[f"step{st}_{f}_digest"] = digest(sim.get_field(f))
+        rec[f"step{st}_counts"] = sim.cell_counts()
+        rec[f"step{st}_energy"] = sim.energy_reference()
+        rec[f"step{st}_particles_digest"] = digest(particle_table(sim.particles()))
+    for f in FIELDS:
+        rec[f"final_{f}"] = sim.get_field(f)
+    np.savez_compressed(os.path.join(OUT, "ref_c0.npz"), **rec)
+
+
+if __name__ == "__main__":
+    if not RefSim.available():
+        sys.exit("oracle/_ref/libref0buf.so missing: run oracle/build_ref.sh where the reference sources exist")
+    make_small()
+    make_c0()
+    for f in ("ref_small.npz", "ref_c0.npz"):
+        print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
