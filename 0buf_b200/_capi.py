@@ -59,6 +59,8 @@ SIGNATURES = {
     "pic_destroy": (C.c_int, [H]),
     "pic_load_particles": (C.c_int, [H, C.c_int, C.c_int64] + [D] * 6 + [I64]),
     "pic_load_particles_device": (C.c_int, [H, C.c_int, C.c_int64] + [C.c_void_p] * 6 + [I64]),
+    "pic_load_particles_cells": (C.c_int, [H, C.c_int, C.c_int64, C.c_void_p] + [C.c_void_p] * 6 + [I64]),
+    "pic_get_particles_cells": (C.c_int, [H, C.c_int, C.c_int64, C.c_void_p] + [C.c_void_p] * 6 + [I64]),
     "pic_init_species_device": (C.c_int, [H, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                           C.c_uint64]),
     "pic_init_species_host": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,

@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <functional>
 #include "pic0buf.h"
 #include "pic_internal.cuh"
 #include "pic_kernels.cuh"
@@ -42,8 +43,9 @@ struct pic_handle {
     int status;
     char err[256];
     int64_t counters[4];
-    float timings[4];
-    cudaEvent_t ev[5];
+    float timings[5];
+    cudaEvent_t ev[6];
+    int64_t launches;  // kernels launched by the current/last step
     int timed;
     int kin_valid;  // st->kinetic holds the kinetic energy of the current momenta
 };
@@ -160,8 +162,9 @@ int ensure_outbox(pic_handle *h) {
 }
 
 // flat device list (cell computed, -1 = rejected) -> bins of species s
-int build_bins(pic_handle *h, int s, int64_t n, int *cell, const double *x, const double *y, const double *z,
-               const double *px, const double *py, const double *pz, int64_t *inserted) {
+using ScatterFn = std::function<cudaError_t(const SpeciesView &, int *)>;
+
+int build_bins_with(pic_handle *h, int s, int64_t n, int *cell, const ScatterFn &scatter, int64_t *inserted) {
     const Grid &g = h->g;
     int *tc = nullptr;
     CK(cudaMalloc(&tc, g.ntiles * sizeof(int)), "alloc tile counts");
@@ -173,7 +176,7 @@ int build_bins(pic_handle *h, int s, int64_t n, int *cell, const double *x, cons
     int rc = alloc_species(h, s, counts);
     if (rc) { cudaFree(tc); return rc; }
     CK(cudaMemsetAsync(tc, 0, g.ntiles * sizeof(int), h->stream), "memset");
-    CK(scatter_to_bins(g, h->mixed, n, cell, x, y, z, px, py, pz, h->sp[s].v, tc, h->stream), "scatter");
+    CK(scatter(h->sp[s].v, tc), "scatter");
     CK(cudaMemcpyAsync(h->sp[s].v.tile_count, tc, g.ntiles * sizeof(int), cudaMemcpyDeviceToDevice, h->stream),
        "tile counts");
     CK(cudaStreamSynchronize(h->stream), "sync");
@@ -183,6 +186,16 @@ int build_bins(pic_handle *h, int s, int64_t n, int *cell, const double *x, cons
     if (inserted) *inserted = tot;
     h->kin_valid = 0;
     return ensure_outbox(h);
+}
+
+int build_bins(pic_handle *h, int s, int64_t n, int *cell, const double *x, const double *y, const double *z,
+               const double *px, const double *py, const double *pz, int64_t *inserted) {
+    const Grid &g = h->g;
+    int mixed = h->mixed;
+    cudaStream_t st = h->stream;
+    return build_bins_with(h, s, n, cell, [&](const SpeciesView &v, int *fill) {
+        return scatter_to_bins(g, mixed, n, cell, x, y, z, px, py, pz, v, fill, st);
+    }, inserted);
 }
 
 int load_device(pic_handle *h, int s, int64_t n, const double *x, const double *y, const double *z,
@@ -242,11 +255,16 @@ int check_status(pic_handle *h) {
     h->counters[0] = (int64_t)st.moved;
     h->counters[1] = (int64_t)st.dropped;
     h->counters[2] = (int64_t)st.duplicated;
-    if (st.flags & ST_STENCIL)
-        return set_err(h, PIC_ERR_STENCIL, "a particle moved more than half a cell in one step (stencil left the tile)");
-    if (st.flags & ST_NAN) return set_err(h, PIC_ERR_NAN, "non-finite momentum after the push");
-    if (st.flags & ST_BADCELL) return set_err(h, PIC_ERR_STATE, "particle bins are inconsistent");
-    if (st.flags & ST_OUTBOX) return set_err(h, PIC_ERR_OUTBOX, "migration outbox overflowed; raise outbox_fraction");
+    char msg[200];
+    const unsigned fatal = ST_STENCIL | ST_NAN | ST_BADCELL | ST_OUTBOX;
+    if (st.flags & fatal) {
+        int code = (st.flags & ST_NAN) ? PIC_ERR_NAN
+                   : (st.flags & ST_STENCIL) ? PIC_ERR_STENCIL
+                   : (st.flags & ST_BADCELL) ? PIC_ERR_STATE : PIC_ERR_OUTBOX;
+        snprintf(msg, sizeof(msg), "%s (status flags 0x%x: 1 stencil, 2 outbox, 4 holes, 8 nan, 16 tile full, 32 bins)",
+                 pic_error_string(code), st.flags);
+        return set_err(h, code, msg);
+    }
     if (st.flags & ST_TILE_FULL) {
         unsigned n_out = st.out_count < h->out_cap ? st.out_count : h->out_cap;
         for (int s = 0; s < h->cfg.nspecies; s++) {
@@ -287,6 +305,7 @@ int do_b_half(pic_handle *h) {
     if (!h->mixed) yee_b_half_plain(h->g, (double *const *)h->f, h->stream);
     else yee_b_half_mixed(h->g, (float *const *)&h->f[PIC_EX], (float *const *)&h->f[PIC_HX], h->stream);
     CK(cudaGetLastError(), "b_half");
+    h->launches += 1;
     return PIC_OK;
 }
 
@@ -297,7 +316,10 @@ int do_push_deposit(pic_handle *h) {
     for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(h->f[PIC_JX + c], 0, nodes * sizeof(double), h->stream), "zero J");
     CK(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), h->stream), "reset status");
     StepParams p = make_params(h);
+    cudaEventRecord(h->ev[2], h->stream);
     CK(h->mixed ? launch_push_mixed(p, h->stream) : launch_push_plain(p, h->stream), "push_deposit");
+    cudaEventRecord(h->ev[3], h->stream);
+    h->launches += 1;
     h->kin_valid = 1;
     return PIC_OK;
 }
@@ -312,6 +334,7 @@ int do_b_complete(pic_handle *h) {
     if (!h->mixed) yee_b_complete_plain(h->g, (double *const *)h->f, h->stream);
     else yee_b_half_mixed(h->g, (float *const *)&h->f[PIC_EX], (float *const *)&h->f[PIC_HX], h->stream);
     CK(cudaGetLastError(), "b_complete");
+    h->launches += 1;
     return PIC_OK;
 }
 
@@ -321,6 +344,7 @@ int do_e_update(pic_handle *h) {
         yee_e_update_mixed(h->g, (float *const *)&h->f[PIC_EX], (float *const *)&h->f[PIC_HX],
                            (double *const *)&h->f[PIC_JX], h->stream);
     CK(cudaGetLastError(), "e_update");
+    h->launches += 1;
     return PIC_OK;
 }
 
@@ -331,12 +355,14 @@ int do_e_ghosts(pic_handle *h) {
     else
         e_ghosts_mixed(h->g, (float *)h->f[PIC_EX], (float *)h->f[PIC_EY], (float *)h->f[PIC_EZ], per, h->stream);
     CK(cudaGetLastError(), "e_ghosts");
+    h->launches += 2;
     return PIC_OK;
 }
 
 int do_j_fold(pic_handle *h) {
     j_fold(h->g, (double *)h->f[PIC_JX], (double *)h->f[PIC_JY], (double *)h->f[PIC_JZ], h->stream);
     CK(cudaGetLastError(), "j_fold");
+    h->launches += 3;
     return PIC_OK;
 }
 
@@ -422,7 +448,7 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
     auto fail = [&](cudaError_t e) { pic_destroy(h); return e == cudaErrorMemoryAllocation ? PIC_ERR_NOMEM : (int)e; };
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e) { delete h; return (int)e; }
-    for (int i = 0; i < 5; i++) cudaEventCreate(&h->ev[i]);
+    for (int i = 0; i < 6; i++) cudaEventCreate(&h->ev[i]);
     size_t nodes = g.nodes_pitched();
     for (int fi = 0; fi < PIC_FIELD_COUNT; fi++) {
         size_t es = sizeof(double);
@@ -431,15 +457,18 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
             if (fi < PIC_JX) es = sizeof(float);
         }
         if ((e = cudaMalloc(&h->f[fi], nodes * es)) != cudaSuccess) return fail(e);
-        if ((e = cudaMemset(h->f[fi], 0, nodes * es)) != cudaSuccess) return fail(e);
+        // on the handle's stream: the legacy-stream cudaMemset does not order
+        // before work on a non-blocking stream
+        if ((e = cudaMemsetAsync(h->f[fi], 0, nodes * es, h->stream)) != cudaSuccess) return fail(e);
     }
     if ((e = cudaMalloc(&h->dense, g.nodes_ref() * sizeof(double))) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&h->st, sizeof(DevStatus))) != cudaSuccess) return fail(e);
-    if ((e = cudaMemset(h->st, 0, sizeof(DevStatus))) != cudaSuccess) return fail(e);
+    if ((e = cudaMemsetAsync(h->st, 0, sizeof(DevStatus), h->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaMallocHost(&h->st_host, sizeof(DevStatus))) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&h->dred, 8 * sizeof(double))) != cudaSuccess) return fail(e);
     if ((e = cudaMallocHost(&h->hred, 8 * sizeof(double))) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&h->dcounts, (size_t)g.ncells() * sizeof(int))) != cudaSuccess) return fail(e);
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return fail(e);
     *out = h;
     return PIC_OK;
 }
@@ -458,7 +487,7 @@ int pic_destroy(pic_handle *h) {
     if (h->dred) cudaFree(h->dred);
     if (h->hred) cudaFreeHost(h->hred);
     if (h->dcounts) cudaFree(h->dcounts);
-    for (int i = 0; i < 5; i++)
+    for (int i = 0; i < 6; i++)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -489,6 +518,79 @@ int pic_load_particles_device(pic_handle *h, int species, int64_t n, const doubl
     int rc = set_device(h);
     if (rc) return rc;
     return load_device(h, species, n, x, y, z, px, py, pz, inserted);
+}
+
+int pic_load_particles_cells(pic_handle *h, int species, int64_t n, const int32_t *cell, const float *ox,
+                             const float *oy, const float *oz, const float *px, const float *py, const float *pz,
+                             int64_t *inserted) {
+    if (!h || species < 0 || species >= h->cfg.nspecies || n < 0) return set_err(h, PIC_ERR_ARG, "bad argument");
+    if (n > 0 && (!cell || !ox || !oy || !oz || !px || !py || !pz)) return set_err(h, PIC_ERR_ARG, "null array");
+    int rc = set_device(h);
+    if (rc) return rc;
+    size_t N = (size_t)(n > 0 ? n : 1);
+    float *buf = nullptr;
+    int *rc_cell = nullptr, *icell = nullptr;
+    CK(cudaMalloc(&buf, N * 6 * sizeof(float)), "alloc load buffer");
+    CK(cudaMalloc(&rc_cell, N * sizeof(int)), "alloc load buffer");
+    CK(cudaMalloc(&icell, N * sizeof(int)), "alloc load buffer");
+    const float *src[6] = {ox, oy, oz, px, py, pz};
+    if (n > 0) {
+        for (int a = 0; a < 6; a++)
+            CK(cudaMemcpyAsync(buf + a * N, src[a], (size_t)n * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+               "H2D particles");
+        CK(cudaMemcpyAsync(rc_cell, cell, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, h->stream), "H2D cells");
+    }
+    const float *fo[6] = {buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N};
+    CK(place_particles_cells(h->g, n, rc_cell, fo[0], fo[1], fo[2], icell, h->stream), "place");
+    const Grid &g = h->g;
+    int mixed = h->mixed;
+    cudaStream_t st = h->stream;
+    rc = build_bins_with(h, species, n, icell, [&](const SpeciesView &v, int *fill) {
+        return scatter_to_bins_f(g, mixed, n, icell, fo[0], fo[1], fo[2], fo[3], fo[4], fo[5], v, fill, st);
+    }, inserted);
+    cudaFree(buf);
+    cudaFree(rc_cell);
+    cudaFree(icell);
+    return rc;
+}
+
+int pic_get_particles_cells(pic_handle *h, int species, int64_t cap, int32_t *cell, float *ox, float *oy, float *oz,
+                            float *px, float *py, float *pz, int64_t *n) {
+    if (!h || species < 0 || species >= h->cfg.nspecies) return set_err(h, PIC_ERR_ARG, "bad argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    const Grid &g = h->g;
+    if (!h->sp[species].loaded) { if (n) *n = 0; return PIC_OK; }
+    SpeciesView &v = h->sp[species].v;
+    std::vector<int> counts(g.ntiles);
+    CK(cudaMemcpyAsync(counts.data(), v.tile_count, g.ntiles * sizeof(int), cudaMemcpyDeviceToHost, h->stream), "counts");
+    CK(cudaStreamSynchronize(h->stream), "sync");
+    std::vector<int64_t> dstart(g.ntiles + 1);
+    int64_t acc = 0;
+    for (int t = 0; t < g.ntiles; t++) { dstart[t] = acc; acc += counts[t]; }
+    dstart[g.ntiles] = acc;
+    if (n) *n = acc;
+    if (acc > cap) return set_err(h, PIC_ERR_ARG, "capacity too small");
+    if (acc == 0) return PIC_OK;
+    size_t N = (size_t)acc;
+    float *buf = nullptr;
+    int *dcell = nullptr;
+    int64_t *dd = nullptr;
+    CK(cudaMalloc(&buf, N * 6 * sizeof(float)), "alloc");
+    CK(cudaMalloc(&dcell, N * sizeof(int)), "alloc");
+    CK(cudaMalloc(&dd, (g.ntiles + 1) * sizeof(int64_t)), "alloc");
+    CK(cudaMemcpyAsync(dd, dstart.data(), (g.ntiles + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream), "H2D");
+    CK(gather_from_bins_f(g, h->mixed, v, dd, dcell, buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N,
+                          h->stream), "gather");
+    float *dst[6] = {ox, oy, oz, px, py, pz};
+    for (int a = 0; a < 6; a++)
+        if (dst[a]) CK(cudaMemcpyAsync(dst[a], buf + a * N, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "D2H");
+    if (cell) CK(cudaMemcpyAsync(cell, dcell, N * sizeof(int), cudaMemcpyDeviceToHost, h->stream), "D2H");
+    CK(cudaStreamSynchronize(h->stream), "sync");
+    cudaFree(buf);
+    cudaFree(dcell);
+    cudaFree(dd);
+    return PIC_OK;
 }
 
 int pic_init_species_device(pic_handle *h, int species, int ppc, double drift_x, double drift_y, double drift_z,
@@ -588,22 +690,28 @@ int pic_step(pic_handle *h, int nt) {
     if (!h) return PIC_ERR_ARG;
     int rc = set_device(h);
     if (rc) return rc;
+    h->launches = 0;
     cudaEventRecord(h->ev[0], h->stream);
     if ((rc = do_b_half(h))) return rc;
     cudaEventRecord(h->ev[1], h->stream);
-    if ((rc = do_push_deposit(h))) return rc;
-    cudaEventRecord(h->ev[2], h->stream);
+    if ((rc = do_push_deposit(h))) return rc;  // records ev[2], ev[3] around the kernel
     StepParams p = make_params(h);
     CK(launch_insert(p, h->stream), "insert");
-    cudaEventRecord(h->ev[3], h->stream);
+    h->launches += 2;
+    cudaEventRecord(h->ev[4], h->stream);
     if ((rc = do_j_fold(h))) return rc;
     if ((rc = do_b_complete(h))) return rc;
     if ((rc = do_e_update(h))) return rc;
     if ((rc = do_e_ghosts(h))) return rc;
-    cudaEventRecord(h->ev[4], h->stream);
+    cudaEventRecord(h->ev[5], h->stream);
     rc = check_status(h);
+    h->counters[3] = h->launches;
     if (!rc) {
-        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&h->timings[i], h->ev[i], h->ev[i + 1]);
+        cudaEventElapsedTime(&h->timings[0], h->ev[0], h->ev[1]);
+        cudaEventElapsedTime(&h->timings[1], h->ev[2], h->ev[3]);
+        cudaEventElapsedTime(&h->timings[2], h->ev[3], h->ev[4]);
+        cudaEventElapsedTime(&h->timings[3], h->ev[4], h->ev[5]);
+        cudaEventElapsedTime(&h->timings[4], h->ev[0], h->ev[5]);
         h->timed = 1;
     }
     return rc;
@@ -784,9 +892,9 @@ int pic_step_counters(pic_handle *h, int64_t *out4) {
     return PIC_OK;
 }
 
-int pic_step_timings(pic_handle *h, float *out4) {
-    if (!h || !out4) return PIC_ERR_ARG;
-    for (int i = 0; i < 4; i++) out4[i] = h->timings[i];
+int pic_step_timings(pic_handle *h, float *out5) {
+    if (!h || !out5) return PIC_ERR_ARG;
+    for (int i = 0; i < 5; i++) out5[i] = h->timings[i];
     return h->timed ? PIC_OK : PIC_ERR_STATE;
 }
 

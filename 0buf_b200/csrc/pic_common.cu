@@ -76,6 +76,68 @@ __global__ void k_scatter(Grid g, int mixed, int64_t n, const int *__restrict__ 
     }
 }
 
+// native-layout load: reference cell number -> interior cell (or -1)
+__global__ void k_place_cells(Grid g, int64_t n, const int *__restrict__ ref_cell, const float *__restrict__ ox,
+                              const float *__restrict__ oy, const float *__restrict__ oz, int *__restrict__ cell) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int r = ref_cell[p];
+    int c = -1;
+    if (r >= 0 && (size_t)r < g.nodes_ref()) {
+        int k = r % g.NZ, l = (r / g.NZ) % g.NY, i = r / (g.NZ * g.NY);
+        bool off = ox[p] >= 0.f && ox[p] < 1.f && oy[p] >= 0.f && oy[p] < 1.f && oz[p] >= 0.f && oz[p] < 1.f;
+        if (i < g.nx && l < g.ny && k < g.nz && off) c = g.cell_of(i, l, k);
+    }
+    cell[p] = c;
+}
+
+__global__ void k_scatter_f(Grid g, int mixed, int64_t n, const int *__restrict__ cell, const float *__restrict__ ox,
+                            const float *__restrict__ oy, const float *__restrict__ oz, const float *__restrict__ px,
+                            const float *__restrict__ py, const float *__restrict__ pz, SpeciesView S, int *fill) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int c = cell[p];
+    if (c < 0) return;
+    int i, l, k;
+    cell_ijk(g, c, i, l, k);
+    int t = g.tile_of_cell(i, l, k);
+    int slot = S.tile_start[t] + atomicAdd(&fill[t], 1);
+    S.cell[slot] = c;
+    if (mixed) {
+        S.ox[slot] = ox[p]; S.oy[slot] = oy[p]; S.oz[slot] = oz[p];
+        S.fx[slot] = px[p]; S.fy[slot] = py[p]; S.fz[slot] = pz[p];
+    } else {
+        S.x[slot] = ((double)i + (double)ox[p]) * g.hx;
+        S.y[slot] = ((double)l + (double)oy[p]) * g.hy;
+        S.z[slot] = ((double)k + (double)oz[p]) * g.hz;
+        S.px[slot] = px[p]; S.py[slot] = py[p]; S.pz[slot] = pz[p];
+    }
+}
+
+__global__ void k_gather_f(Grid g, int mixed, SpeciesView S, const int64_t *__restrict__ dense_start, int *cell,
+                           float *ox, float *oy, float *oz, float *px, float *py, float *pz) {
+    int t = blockIdx.x;
+    int start = S.tile_start[t], n = S.tile_count[t];
+    int64_t d0 = dense_start[t];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        int slot = start + j;
+        int c = S.cell[slot];
+        int64_t d = d0 + j;
+        int i = 0, l = 0, k = 0;
+        if (c >= 0) cell_ijk(g, c, i, l, k);
+        cell[d] = c < 0 ? -1 : (int)(((size_t)i * g.NY + l) * g.NZ + k);
+        if (mixed) {
+            ox[d] = S.ox[slot]; oy[d] = S.oy[slot]; oz[d] = S.oz[slot];
+            px[d] = S.fx[slot]; py[d] = S.fy[slot]; pz[d] = S.fz[slot];
+        } else {
+            ox[d] = to_offset(S.x[slot], i, g.hx);
+            oy[d] = to_offset(S.y[slot], l, g.hy);
+            oz[d] = to_offset(S.z[slot], k, g.hz);
+            px[d] = (float)S.px[slot]; py[d] = (float)S.py[slot]; pz[d] = (float)S.pz[slot];
+        }
+    }
+}
+
 // Arrivals of the migration (replaces GPU_ArrangeFlights' Insert, kernels.cu:316-370):
 // every outbox entry is appended to its destination tile.  Entries that fit
 // are marked done (cell = -1); the rest stay for a rebin.
@@ -319,6 +381,27 @@ cudaError_t scatter_to_bins(const Grid &g, int mixed, int64_t n, const int *cell
                             int *fill, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(g, mixed, n, cell, x, y, z, px, py, pz, sv, fill);
+    return cudaGetLastError();
+}
+
+cudaError_t place_particles_cells(const Grid &g, int64_t n, const int *ref_cell, const float *ox, const float *oy,
+                                  const float *oz, int *cell_out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_place_cells<<<blocks_for(n, 256), 256, 0, s>>>(g, n, ref_cell, ox, oy, oz, cell_out);
+    return cudaGetLastError();
+}
+
+cudaError_t scatter_to_bins_f(const Grid &g, int mixed, int64_t n, const int *cell, const float *ox, const float *oy,
+                              const float *oz, const float *px, const float *py, const float *pz, SpeciesView sv,
+                              int *fill, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_scatter_f<<<blocks_for(n, 256), 256, 0, s>>>(g, mixed, n, cell, ox, oy, oz, px, py, pz, sv, fill);
+    return cudaGetLastError();
+}
+
+cudaError_t gather_from_bins_f(const Grid &g, int mixed, SpeciesView sv, const int64_t *dense_start, int *cell,
+                               float *ox, float *oy, float *oz, float *px, float *py, float *pz, cudaStream_t s) {
+    k_gather_f<<<g.ntiles, 256, 0, s>>>(g, mixed, sv, dense_start, cell, ox, oy, oz, px, py, pz);
     return cudaGetLastError();
 }
 

@@ -27,6 +27,14 @@ cudaError_t launch_push_mixed(const StepParams &p, cudaStream_t s);
 // form-independent (pic_common.cu, FP64 parts with -fmad=false)
 cudaError_t launch_insert(const StepParams &p, cudaStream_t s);
 cudaError_t cell_histogram(const StepParams &p, int *counts, cudaStream_t s);
+// native 28-byte layout (reference cell number, FP32 offsets and momenta)
+cudaError_t place_particles_cells(const Grid &g, int64_t n, const int *ref_cell, const float *ox, const float *oy,
+                                  const float *oz, int *cell_out, cudaStream_t s);
+cudaError_t scatter_to_bins_f(const Grid &g, int mixed, int64_t n, const int *cell, const float *ox, const float *oy,
+                              const float *oz, const float *px, const float *py, const float *pz, SpeciesView sv,
+                              int *fill, cudaStream_t s);
+cudaError_t gather_from_bins_f(const Grid &g, int mixed, SpeciesView sv, const int64_t *dense_start, int *cell,
+                               float *ox, float *oy, float *oz, float *px, float *py, float *pz, cudaStream_t s);
 // flat device list -> per-tile counts of valid particles (cell >= 0)
 cudaError_t tile_histogram(const Grid &g, int64_t n, const int *cell, int *tile_counts, cudaStream_t s);
 // flat FP64 list -> bins of one species (plain or mixed), fill[] = running counts

@@ -200,12 +200,13 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
 
             // ---- CurrentToMesh (cell.h:1306-1422) in cell units
             {
+                // cell-centre index of the end point from the same exact float
+                // thresholds as i1 (x + 2.5 rounded in FP32 would put a point one
+                // ulp below a centre plane on the far side of it)
                 int i1[3] = {i1x, i1y, i1z}, i2[3];
 #pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    float tt = xe[d] + 2.5f;
-                    i2[d] = tt > 0.f ? (int)tt : 0;
-                }
+                for (int d = 0; d < 3; d++)
+                    i2[d] = 2 + (xe[d] >= 0.5f) + (xe[d] >= 1.5f) - (xe[d] < -0.5f);
                 if (i2[0] < 2 || i2[0] > 3 || i2[1] < 2 || i2[1] > 3 || i2[2] < 2 || i2[2] > 3) {
                     bad |= ST_STENCIL;
                 } else {

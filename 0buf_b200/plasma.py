@@ -89,6 +89,25 @@ class PicSimulation:
                  "pic_load_particles")
         return ins.value
 
+    def load_particles_cells(self, species: int, cell, ox, oy, oz, px, py, pz) -> int:
+        """Native 28-byte layout: reference cell number, FP32 offsets and momenta.
+        Arrays may be numpy arrays or pinned host torch tensors (anything with
+        a host data pointer: ``.ctypes.data`` or ``.data_ptr()``)."""
+        ptrs = [_host_ptr(a) for a in (cell, ox, oy, oz, px, py, pz)]
+        n = _length(cell)
+        ins = C.c_int64(0)
+        self._ck(self.lib.pic_load_particles_cells(self.h, species, n, *ptrs, C.byref(ins)),
+                 "pic_load_particles_cells")
+        return ins.value
+
+    def get_particles_cells(self, species: int, out) -> int:
+        """Exports one species into ``out`` = (cell, ox, oy, oz, px, py, pz) host arrays."""
+        ptrs = [_host_ptr(a) for a in out]
+        got = C.c_int64(0)
+        self._ck(self.lib.pic_get_particles_cells(self.h, species, _length(out[0]), *ptrs, C.byref(got)),
+                 "pic_get_particles_cells")
+        return got.value
+
     def init_species(self, species: int, ppc: int, drift=(0.0, 0.0, 0.0), vth: float = 0.0, seed: int = 0):
         self._ck(self.lib.pic_init_species_device(self.h, species, ppc, *[float(d) for d in drift], float(vth),
                                                   int(seed)), "pic_init_species_device")
@@ -166,7 +185,8 @@ class PicSimulation:
         return c
 
     def timings(self) -> np.ndarray:
-        t = np.zeros(4, np.float32)
+        """[b_half, push kernel, migration arrivals, second field half, whole step] in ms."""
+        t = np.zeros(5, np.float32)
         self.lib.pic_step_timings(self.h, t.ctypes.data_as(_capi.F))
         return t
 
@@ -174,6 +194,17 @@ class PicSimulation:
         v = np.zeros(4, np.int64)
         self._ck(self.lib.pic_layout_info(self.h, v.ctypes.data_as(_capi.I64)), "pic_layout_info")
         return dict(tiles=int(v[0]), slots=int(v[1]), bytes_per_particle=int(v[2]), nodes=int(v[3]))
+
+
+def _host_ptr(a):
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a.data_ptr())  # torch tensor on the host
+
+
+def _length(a) -> int:
+    return int(a.size if isinstance(a, np.ndarray) else a.numel())
 
 
 def host_species(cells, lengths, species_index: int, ppc: int, drift=(0.0, 0.0, 0.0), vth: float = 0.0,

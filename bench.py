@@ -1,0 +1,466 @@
+"""Benchmark of the B200 PIC time step: particle-steps/s.
+
+Workload (default): 512x128x128 cells, 32 particles per cell per species,
+3 species (805,306,368 particles), FP32 mixed form; synthetic seeded
+uniform/Maxwellian inputs.  One "step" is one full PIC step (B half step,
+push + deposit, migration, J fold, B completion, E update, E ghosts) over all
+particles.  Inputs are larger than L2 (22.5 GB of particles), so no L2 flush
+is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU (torchrun); the path has no exchange step on
+one GPU's domain, so the ranks run independent replicas (different seeds),
+"scaling": "weak"; value = all ranks' particle-steps / max-over-ranks time.
+
+--impl reference times the reference's own CPU implementation (the reference's
+functions compiled for the host, oracle/_ref) on the host cores at its own
+CPU-runnable case (32x4x4 cells), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s, FP32-mixed vs FP64 on B200 at stated error; adjoint/fwd time"
+UNIT = "particle-steps/s"
+# algorithmic bytes per particle-step of the push/deposit kernel: read + write
+# of one particle (mixed: int32 cell + 3 FP32 offsets + 3 FP32 momenta = 28 B;
+# plain: int32 cell + 3 FP64 positions + 3 FP64 momenta = 52 B)
+BYTES_PER_PARTICLE_STEP = {"fp32": 56, "fp64": 104}
+# algorithmic bytes per Yee cell-update: read E, B, J and write E, B
+BYTES_PER_CELL_UPDATE = {"fp32": 72, "fp64": 120}
+# DRAM bytes per particle of the push kernel from one ncu capture
+# (profiles/push_mixed_c2_ncu.md); None until measured
+NCU_TRAFFIC_PER_PARTICLE = {"fp32": None, "fp64": None}
+KERNELS_PER_STEP_NOTE = "b_half, push, insert, clamp, j_fold x3, b_complete, e_update, e_ghosts x2"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- dist
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self, backend: str | None = None):
+        if self.world <= 1:
+            return
+        import torch
+        import torch.distributed as dist
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if backend == "nccl":
+            torch.cuda.set_device(self.local)
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        self.backend = backend
+        self.pg = True
+
+    def _t(self, x):
+        import torch
+        dev = "cuda" if getattr(self, "backend", "") == "nccl" else "cpu"
+        return torch.tensor([float(x)], dtype=torch.float64, device=dev)
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return float(x)
+        import torch.distributed as dist
+        t = self._t(x)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return float(x)
+        import torch.distributed as dist
+        t = self._t(x)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            if getattr(self, "backend", "") == "nccl":
+                dist.barrier(device_ids=[self.local])
+            else:
+                dist.barrier()
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+            self.pg = False
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int | None = None):
+        self.lines = []
+        self.proc = None
+        self.gpu_index = gpu_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append(dict(idx=int(f[0]), sm=float(f[1]), smax=float(f[2]), reasons=f[5:9]))
+            except ValueError:
+                continue
+        if self.gpu_index is not None and any(r["idx"] == self.gpu_index for r in rows):
+            rows = [r for r in rows if r["idx"] == self.gpu_index]
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r["reasons"]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------- our arm
+def make_sim(pkg, cfg, form, device, seed_base):
+    cells, h, tau, ppc = cfg["cells"], cfg["h"], cfg["tau"], cfg["ppc"]
+    box = tuple(c * h for c in cells)
+    sim = pkg.PicSimulation(cells, box, tau, pkg.configs.species_table(ppc), precision=form, device=device)
+    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
+        sim.init_species(i, ppc, s["drift"], s["vth"], seed_base + i)
+    return sim
+
+
+def timed_steps(sim, K, torch):
+    """K steps between CUDA events recorded on the library's stream."""
+    stream = torch.cuda.ExternalStream(sim.lib.pic_stream(sim.h))
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    push_ms, b_ms, mig_ms, f2_ms, launches = [], [], [], [], 0
+    t0.record(stream)
+    for k in range(K):
+        sim.step(k + 1)
+        t = sim.timings()
+        b_ms.append(float(t[0]))
+        push_ms.append(float(t[1]))
+        mig_ms.append(float(t[2]))
+        f2_ms.append(float(t[3]))
+        launches += int(sim.counters()[3])
+    t1.record(stream)
+    t1.synchronize()
+    return t0.elapsed_time(t1), dict(b_half=b_ms, push=push_ms, migrate=mig_ms, fields2=f2_ms), launches
+
+
+def run_ours(args, dist):
+    import numpy as np
+    import torch
+
+    pkg = importlib.import_module("0buf_b200")
+    cfg = dict(pkg.configs.CONFIGS[args.config])
+    if args.cells:
+        cfg["cells"] = tuple(int(c) for c in args.cells.split(","))
+        args.config = "custom"
+    if args.ppc:
+        cfg["ppc"] = args.ppc
+        args.config = "custom"
+    form = args.form or cfg["precision"]
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    K, W = args.steps, args.warmup
+    seed_base = 1000 * dist.rank
+    cells = cfg["cells"]
+    ncell = int(np.prod(cells))
+
+    sim = make_sim(pkg, cfg, form, dev, seed_base)
+    n_local = sim.num_particles()
+    for w in range(W):
+        sim.step(w + 1)
+    dist.barrier()
+    sampler = ClockSampler(dev) if dist.rank == 0 else None
+    if sampler:
+        sampler.start()
+    elapsed_ms, phases, launches = timed_steps(sim, K, torch)
+    clocks = sampler.stop() if sampler else None
+    dist.barrier()
+    t_max = dist.max(elapsed_ms)
+    n_total = dist.sum(n_local)
+    value = n_total * K / (t_max / 1e3)
+    push_avg_ms = statistics.mean(phases["push"])
+    yee_ms = statistics.mean(phases["b_half"]) + statistics.mean(phases["fields2"])
+    layout = sim.layout()
+    energy_last = sim.energy().tolist()
+    sim.close()
+    del sim
+
+    peak, peak_kind = peaks()
+    bpp = BYTES_PER_PARTICLE_STEP[form]
+    achieved = bpp * n_local / (push_avg_ms / 1e3) / 1e9
+    traffic = NCU_TRAFFIC_PER_PARTICLE[form]
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "traffic": (round(traffic * n_local) if traffic else None),
+                "kernel": f"k_push_{'mixed' if form == 'fp32' else 'plain'}",
+                "algorithmic_bytes_per_launch": bpp * n_local, "avg_launch_ms": round(push_avg_ms, 4)}
+    yee = {"cell_updates_per_s": round(ncell / (yee_ms / 1e3), 1), "ms_per_step": round(yee_ms, 4),
+           "achieved_gbs": round(BYTES_PER_CELL_UPDATE[form] * ncell / (yee_ms / 1e3) / 1e9, 1)}
+    yee["frac"] = round(yee["achieved_gbs"] / peak, 4)
+
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
+        "ms_per_step": round(t_max / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if form == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {cells[0]}x{cells[1]}x{cells[2]} cells, {cfg['ppc']} particles/cell/"
+                               f"species x 3 species = {int(n_total / dist.world):,} particles per GPU, "
+                               f"{'FP32 mixed form (FP64 global J)' if form == 'fp32' else 'FP64 plain form'}",
+                   "cells": list(cells), "ppc": cfg["ppc"], "species": 3, "form": form, "tau": cfg["tau"],
+                   "h": cfg["h"], "parallelism": f"replicas x{dist.world}",
+                   "l2": f"inputs larger than L2 ({layout['bytes_per_particle'] * n_local / 1e9:.1f} GB of particles)"},
+        "roofline": roofline,
+        "yee": yee,
+        "phases_ms": {k: round(statistics.mean(v), 4) for k, v in phases.items()},
+        "gpu_launches": launches,
+        "launches_note": KERNELS_PER_STEP_NOTE,
+        "energy_after": energy_last,
+    }
+    if clocks:
+        out["clocks"] = clocks
+
+    # FP64 plain form at the same configuration (N=1 only): the >= 2x claim
+    if dist.world == 1 and not args.no_plain and form == "fp32":
+        simp = make_sim(pkg, cfg, "fp64", dev, seed_base)
+        for w in range(2):
+            simp.step(w + 1)
+        Kp = max(3, K // 2)
+        ms_p, ph_p, _ = timed_steps(simp, Kp, torch)
+        vp = n_local * Kp / (ms_p / 1e3)
+        pp = statistics.mean(ph_p["push"])
+        out["plain_fp64"] = {"value": round(vp, 1), "ms_per_step": round(ms_p / Kp, 4), "steps": Kp,
+                             "push_ms": round(pp, 4),
+                             "push_achieved_gbs": round(104 * n_local / (pp / 1e3) / 1e9, 1),
+                             "mixed_over_plain": round(value / vp, 3)}
+        simp.close()
+        del simp
+
+    if not args.no_e2e:
+        out["e2e"] = run_e2e(args, dist, pkg, cfg, form, torch, n_local)
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+def run_e2e(args, dist, pkg, cfg, form, torch, n_local):
+    """Same metric through the C ABI from pinned HOST memory: load all species
+    (host->device, 28 B/particle), K steps, one energy read-back per step."""
+    import psutil
+
+    need = 28 * n_local
+    if psutil.virtual_memory().available < 2.5 * need:
+        return {"value": None, "unit": UNIT, "note": f"host RAM below 2.5x the {need / 1e9:.1f} GB of inputs"}
+    K = args.steps
+    dev = dist.local
+    sim = make_sim(pkg, cfg, form, dev, 1000 * dist.rank)
+    host = []
+    for s in range(sim.nspecies):
+        n = sim.num_particles(s)
+        arrs = [torch.empty(n, dtype=torch.int32, pin_memory=True)] + \
+               [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(6)]
+        got = sim.get_particles_cells(s, arrs)
+        assert got == n
+        host.append(arrs)
+    table = pkg.configs.species_table(cfg["ppc"])
+    box = tuple(c * cfg["h"] for c in cfg["cells"])
+    sim.close()
+    del sim
+    torch.cuda.synchronize()
+    dist.barrier()
+    sim = pkg.PicSimulation(cfg["cells"], box, cfg["tau"], table, precision=form, device=dev)
+    stream = torch.cuda.ExternalStream(sim.lib.pic_stream(sim.h))
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    h2d = 0
+    for s, arrs in enumerate(host):
+        sim.load_particles_cells(s, *arrs)
+        h2d += sum(a.numel() * a.element_size() for a in arrs)
+    energies = []
+    for k in range(K):
+        sim.step(k + 1)
+        energies.append(sim.energy())
+    t1.record(stream)
+    t1.synchronize()
+    ms = t0.elapsed_time(t1)
+    sim.close()
+    dist.barrier()
+    t_max = dist.max(ms)
+    n_total = dist.sum(n_local)
+    # per step the library reads back its 72-byte status word and the 64-byte reduction buffer
+    return {"value": round(n_total * K / (t_max / 1e3), 1), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": 72 + 64, "steps": K,
+            "ms_total": round(t_max, 2), "path": "pic_create + pic_load_particles_cells (pinned host) + "
+            "K x (pic_step + pic_energy)"}
+
+
+# ------------------------------------------------------- CPU baselines
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_sim(kind_pref="reference"):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    oracle = importlib.import_module("oracle")
+    if kind_pref == "reference" and oracle.RefSim.available():
+        return oracle.RefSim, "reference"
+    return oracle.OracleSim, "port"
+
+
+def cpu_run(seconds: float, min_steps: int, max_steps: int, threads: int, kind_pref="reference"):
+    """The reference CPU path at its own case (32x4x4 cells, 32 ppc x 3 species)."""
+    import numpy as np
+    pkg = importlib.import_module("0buf_b200")
+    Sim, kind = cpu_sim(kind_pref)
+    cfg = pkg.configs.CONFIGS["c0"]
+    cells, h, tau, ppc = cfg["cells"], cfg["h"], cfg["tau"], cfg["ppc"]
+    box = tuple(c * h for c in cells)
+    sim = Sim(cells, box, tau, threads=threads)
+    table = pkg.configs.species_table(ppc)
+    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
+        arrs = pkg.host_species(cells, box, i, ppc, s["drift"], s["vth"], 0)
+        sim.add_particles(s["sort"], *arrs, table[i][1], s["q_m"])
+    n = sim.num_particles()
+    sim.step()  # warm
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps and (steps < min_steps or time.perf_counter() - t0 < seconds):
+        assert sim.step() == 0
+        steps += 1
+    dt = time.perf_counter() - t0
+    sim.close()
+    return dict(value=round(n * steps / dt, 1), unit=UNIT, cores=threads, kind=kind,
+                sample=f"{steps} steps of the 32x4x4-cell case ({n} particles) with {threads} threads, "
+                       f"{dt:.1f} s; {'reference functions compiled for the host (oracle/_ref)' if kind == 'reference' else 'C restatement (oracle/cpu_pic.c)'}",
+                np=int(np.int64(n)))
+
+
+def cpu_baseline(args):
+    return cpu_run(args.cpu_seconds, 5, 100000, cpu_threads())
+
+
+def run_reference(args):
+    """--impl reference: the reference's own CPU implementation, rank 0 only."""
+    threads = cpu_threads()
+    pkg = importlib.import_module("0buf_b200")
+    Sim, kind = cpu_sim("reference")
+    cfg = pkg.configs.CONFIGS["c0"]
+    cells, h, tau, ppc = cfg["cells"], cfg["h"], cfg["tau"], cfg["ppc"]
+    box = tuple(c * h for c in cells)
+    sim = Sim(cells, box, tau, threads=threads)
+    table = pkg.configs.species_table(ppc)
+    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
+        arrs = pkg.host_species(cells, box, i, ppc, s["drift"], s["vth"], 0)
+        sim.add_particles(s["sort"], *arrs, table[i][1], s["q_m"])
+    n = sim.num_particles()
+    for _ in range(args.warmup):
+        assert sim.step() == 0
+    # each benchmark step: a bounded sample of PIC steps of the case
+    inner = max(1, args.reference_inner)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for _ in range(inner):
+            assert sim.step() == 0
+    dt = time.perf_counter() - t0
+    sim.close()
+    value = n * args.steps * inner / dt
+    sample = (f"{args.steps} x {inner} steps of the 32x4x4-cell case ({n} particles), {threads} threads; "
+              f"{'reference functions compiled for the host (oracle/_ref)' if kind == 'reference' else 'C restatement of the reference (oracle/cpu_pic.c)'}")
+    return {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "c0: 32x4x4 cells, 32 particles/cell/species x 3 species (the reference's "
+                                   "CPU-runnable case; its per-cell 5000-slot containers cannot hold the GPU configs)",
+                       "cells": list(cells), "ppc": ppc},
+            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--form", choices=["fp32", "fp64"], default=None)
+    ap.add_argument("--cells", default=None, help="override cells, e.g. 128,64,64 (profiling cases)")
+    ap.add_argument("--ppc", type=int, default=None, help="override particles per cell per species")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--reference-inner", type=int, default=20)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    dist = Dist()
+    if args.impl == "reference":
+        if dist.rank != 0:
+            return
+        print(json.dumps(run_reference(args)), flush=True)
+        return
+    dist.init()
+    try:
+        out = run_ours(args, dist)
+    finally:
+        dist.barrier()
+        dist.close()
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

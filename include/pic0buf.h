@@ -108,6 +108,18 @@ int pic_load_particles_device(pic_handle *h, int species, int64_t n, const doubl
                               const double *z, const double *px, const double *py, const double *pz,
                               int64_t *inserted);
 
+/* Loads (replaces) one species from HOST arrays in the mixed form's native
+ * layout, 28 bytes per particle: reference cell number (interior cells only),
+ * FP32 in-cell offsets in [0,1) and FP32 momenta.  The plain form forms its
+ * FP64 positions as (i + offset) * h.  Entries with a ghost/out-of-range cell
+ * or an offset outside [0,1) are dropped. */
+int pic_load_particles_cells(pic_handle *h, int species, int64_t n, const int32_t *cell, const float *ox,
+                             const float *oy, const float *oz, const float *px, const float *py, const float *pz,
+                             int64_t *inserted);
+/* Exports one species in the same layout (plain form: offsets rounded to FP32). */
+int pic_get_particles_cells(pic_handle *h, int species, int64_t cap, int32_t *cell, float *ox, float *oy,
+                            float *oz, float *px, float *py, float *pz, int64_t *n);
+
 /* Seeded uniform-in-cell / Maxwellian species generated on the device:
  * ppc particles per interior cell at uniform in-cell offsets, momenta
  * drift + vth * N(0,1) per axis.  Keyed by (seed, species, cell, slot). */
@@ -175,11 +187,12 @@ const char *pic_last_error_string(pic_handle *h);
 const char *pic_error_string(int status);
 /* Per-step counters of the last step: [0] particles moved to another tile,
  * [1] particles no cell accepted (dropped), [2] particles two or more cells
- * accepted (duplicated), [3] tile slots in use (max over tiles, percent). */
+ * accepted (duplicated), [3] kernel launches of the step. */
 int pic_step_counters(pic_handle *h, int64_t *out4);
 /* Timings of the last pic_step in milliseconds (CUDA events on the handle's
- * stream): [0] b_half [1] push_deposit [2] migrate [3] fields second half. */
-int pic_step_timings(pic_handle *h, float *out4);
+ * stream): [0] B half step, [1] the push/deposit kernel alone, [2] migration
+ * arrivals, [3] J fold + B completion + E update + E ghosts, [4] whole step. */
+int pic_step_timings(pic_handle *h, float *out5);
 /* Internal sizes for the roofline: [0] tiles [1] total particle slots
  * [2] bytes per particle (28 mixed / 52 plain) [3] field nodes. */
 int pic_layout_info(pic_handle *h, int64_t *out4);

@@ -240,6 +240,46 @@ def test_mixed_form_tracks_plain(pkg, oracle_mod):
         assert rel_l2(a, b) < 1e-3, f
 
 
+def test_mixed_centre_plane_ulp(pkg):
+    """Offsets one float ulp below a cell-centre plane, moving by less than an
+    ulp-scale step: the deposit must not see a centre crossing (regression:
+    FP32 x + 2.5 rounds 0.49999997 up to the far side, and the split ratio
+    divided by ~0)."""
+    cells, h, tau = (4, 4, 4), 0.1, 0.02
+    sim = pkg.PicSimulation(cells, tuple(c * h for c in cells), tau, [(-1.0, -0.1, 1)], precision="fp32")
+    below = np.nextafter(np.float32(0.5), np.float32(0.0))
+    n = 6
+    ref_cell = np.full(n, (1 * 6 + 1) * 6 + 1, np.int32)  # interior cell (1,1,1), reference numbering
+    ox = np.full(n, below, np.float32)
+    oy = np.array([below, 0.25, 0.75, below, 0.1, 0.9], np.float32)
+    oz = np.full(n, np.float32(0.3))
+    px = np.array([1e-9, 0.0, -1e-9, 1e-7, 0.01, -0.01], np.float32)
+    py = np.array([0.0, 1e-9, 0.0, 1e-8, 0.0, 0.0], np.float32)
+    pz = np.zeros(n, np.float32)
+    assert sim.load_particles_cells(0, ref_cell, ox, oy, oz, px, py, pz) == n
+    for st in range(3):
+        sim.step(st)
+    for f in ("Jx", "Jy", "Jz", "Ex", "Ey", "Ez"):
+        assert np.isfinite(sim.get_field(f)).all(), f
+
+
+def test_mixed_at_scale_stays_finite(pkg):
+    """50M particles, 3 steps: fields and particles stay finite (the rare
+    rounding paths only show up at this size)."""
+    cells, ppc = (128, 64, 64), 32
+    box = tuple(c * 0.1 for c in cells)
+    sim = pkg.PicSimulation(cells, box, 0.02, pkg.configs.species_table(ppc), precision="fp32")
+    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
+        sim.init_species(i, ppc, s["drift"], s["vth"], i)
+    n0 = sim.num_particles()
+    sim.run(3)
+    assert sim.num_particles() == n0
+    for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz"):
+        assert np.isfinite(sim.get_field(f)).all(), f
+    e = sim.energy()
+    assert np.isfinite(e).all() and e[2] > 0
+
+
 def test_plasma_mirror_runs(pkg, oracle_mod):
     """The reference-shaped host surface (Plasma / Step / control points)."""
     P = pkg.Plasma(16, 4, 4, 1.6, 0.4, 0.4, 1.0, 8, 1.0 / 1836.0, 0.02)
