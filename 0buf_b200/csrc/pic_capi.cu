@@ -432,6 +432,10 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
     g.nty = (g.ny + g.ty - 1) / g.ty;
     g.ntz = (g.nz + g.tz - 1) / g.tz;
     g.ntiles = g.ntx * g.nty * g.ntz;
+    auto bits = [](int n) { int b = 0; while ((1 << b) < n) b++; return b; };
+    g.bz = bits(g.nz);
+    g.by = bits(g.ny);
+    if (bits(g.nx) + g.by + g.bz > 31) { delete h; return PIC_ERR_ARG; }  // packed int32 cell index
     for (int s = 0; s < cfg->nspecies; s++) {
         memset(&h->sp[s].v, 0, sizeof(SpeciesView));
         h->sp[s].v.q_m = cfg->species[s].q_m;
@@ -746,7 +750,7 @@ int pic_get_cell_counts(pic_handle *h, int *counts) {
     memset(counts, 0, g.nodes_ref() * sizeof(int));
     for (int i = 0; i < g.nx; i++)
         for (int l = 0; l < g.ny; l++)
-            for (int k = 0; k < g.nz; k++) counts[((size_t)i * g.NY + l) * g.NZ + k] = c[g.cell_of(i, l, k)];
+            for (int k = 0; k < g.nz; k++) counts[((size_t)i * g.NY + l) * g.NZ + k] = c[g.dense_of(i, l, k)];
     return PIC_OK;
 }
 
@@ -807,7 +811,8 @@ int pic_get_particles(pic_handle *h, int species, int64_t cap, double *x, double
         for (size_t j = 0; j < N; j++) {
             int c = hc[j];
             if (c < 0) { cell[j] = -1; continue; }
-            int k = c % g.nz, l = (c / g.nz) % g.ny, i = c / (g.nz * g.ny);
+            int i, l, k;
+            g.cell_ijk(c, i, l, k);
             cell[j] = (int)(((size_t)i * g.NY + l) * g.NZ + k);
         }
     }

@@ -13,11 +13,7 @@ namespace {
 
 constexpr float kOneBelow = 0.99999994f;
 
-__device__ __forceinline__ void cell_ijk(const Grid &g, int cell, int &i, int &l, int &k) {
-    k = cell % g.nz;
-    l = (cell / g.nz) % g.ny;
-    i = cell / (g.nz * g.ny);
-}
+__device__ __forceinline__ void cell_ijk(const Grid &g, int cell, int &i, int &l, int &k) { g.cell_ijk(cell, i, l, k); }
 
 // getPointCell (cell.h:585-598) + Cell::Insert / isPointInCell (cell.h:717,
 // 1754-1768) as used by addParticleListToCells (init.cu:558-592).  Only the
@@ -193,7 +189,10 @@ __global__ void k_cell_hist(StepParams P, int *counts) {
     int start = S.tile_start[t], n = S.tile_count[t];
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
         int c = S.cell[start + j];
-        if (c >= 0 && c < P.g.ncells()) atomicAdd(&counts[c], 1);
+        if (c < 0) continue;
+        int i, l, k;
+        cell_ijk(P.g, c, i, l, k);
+        if (i < P.g.nx && l < P.g.ny && k < P.g.nz) atomicAdd(&counts[P.g.dense_of(i, l, k)], 1);
     }
 }
 
@@ -254,9 +253,9 @@ __global__ void k_init_bins(Grid g, int mixed, SpeciesView S, int species_index,
     int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t total = (int64_t)g.ncells() * ppc;
     if (q >= total) return;
+    // c: dense cell number (i*Ny + l)*Nz + k, the generator's key
     int c = (int)(q / ppc), slot_in_cell = (int)(q % ppc);
-    int i, l, k;
-    cell_ijk(g, c, i, l, k);
+    int k = c % g.nz, l = (c / g.nz) % g.ny, i = c / (g.nz * g.ny);
     int t = g.tile_of_cell(i, l, k);
     int li = i % g.tx, ll = l % g.ty, lk = k % g.tz;
     int ti = i / g.tx, tl = l / g.ty, tk = k / g.tz;
@@ -273,7 +272,7 @@ __global__ void k_init_bins(Grid g, int mixed, SpeciesView S, int species_index,
         p1 = dy + vth * rng_normal(seed, species_index, c, slot_in_cell, 1);
         p2 = dz + vth * rng_normal(seed, species_index, c, slot_in_cell, 2);
     }
-    S.cell[slot] = c;
+    S.cell[slot] = g.cell_of(i, l, k);
     if (!mixed) {
         S.x[slot] = (double)i * g.hx + ox * g.hx;
         S.y[slot] = (double)l * g.hy + oy * g.hy;

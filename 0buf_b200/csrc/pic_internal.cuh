@@ -23,7 +23,7 @@
 namespace pic {
 
 constexpr int kMaxSpecies = PIC_MAX_SPECIES;
-constexpr int kHoleMax = 4096;          // departures per tile per species handled in-kernel
+constexpr int kHoleMax = 1024;          // departures per tile per species handled in-kernel
 constexpr int kPushThreads = 256;
 
 // status flag bits (DevStatus::flags)
@@ -55,16 +55,42 @@ struct Grid {
     int tx, ty, tz;     // cells per tile
     int ntx, nty, ntz;  // tiles per axis
     int ntiles;
+    int bz, by;         // bits of the packed cell index used by k and by l
     double lx, ly, lz, hx, hy, hz, tau;
     __host__ __device__ size_t nodes_pitched() const { return (size_t)NX * NY * pz; }
     __host__ __device__ size_t nodes_ref() const { return (size_t)NX * NY * NZ; }
     __host__ __device__ size_t node(int i, int l, int k) const { return ((size_t)i * NY + l) * pz + k; }
     __host__ __device__ int ncells() const { return nx * ny * nz; }
-    __host__ __device__ int cell_of(int i, int l, int k) const { return (i * ny + l) * nz + k; }
+    // a particle's int32 cell index packs (i, l, k) as bit fields, so the hot
+    // loops decode it with shifts and masks instead of integer division
+    __host__ __device__ int cell_of(int i, int l, int k) const { return (i << (by + bz)) | (l << bz) | k; }
+    __host__ __device__ void cell_ijk(int c, int &i, int &l, int &k) const {
+        k = c & ((1 << bz) - 1);
+        l = (c >> bz) & ((1 << by) - 1);
+        i = c >> (by + bz);
+    }
+    __host__ __device__ int dense_of(int i, int l, int k) const { return (i * ny + l) * nz + k; }
     __host__ __device__ int tile_of_cell(int i, int l, int k) const {
         return ((i / tx) * nty + (l / ty)) * ntz + (k / tz);
     }
 };
+
+// Tile current accumulation in 64-bit fixed point.  Each contribution is
+// rounded to the tile's quantum q = 2^(E-62), where 2^E exceeds
+// bound = 2.5 * sum_s |m_s| * count_s(tile): one particle segment adds at most
+// 1.03 |m| to a node (pqr, cell.h:1578-1616, with |dx| < tau and the stencil
+// in range), two segments per particle, so no tile sum can overflow.  Integer
+// shared-memory atomics are native (no compare-and-swap retry loop) and the
+// sums are exact, so the tile current does not depend on the order in which
+// the threads add.  Rounding: |error| <= q/2 per contribution.
+__device__ __forceinline__ void fx_add(unsigned long long *a, double v, double inv_q) {
+    long long iv = __double2ll_rn(v * inv_q);
+    if (iv) atomicAdd(a, (unsigned long long)iv);
+}
+__device__ __forceinline__ void fx_addf(unsigned long long *a, float v, float inv_q) {
+    long long iv = __float2ll_rn(v * inv_q);
+    if (iv) atomicAdd(a, (unsigned long long)iv);
+}
 
 struct SpeciesView {
     // plain form

@@ -4,8 +4,8 @@
 // re-expressed in cell units so positions never lose resolution with the
 // size of the box: a particle is (int32 cell, FP32 offset in [0,1) per axis,
 // FP32 momentum).  Push, deposit and Yee run in FP32; the deposit
-// pre-reduces each tile's current in shared memory in FP32 and adds the tile
-// into the global J in FP64.
+// pre-reduces each tile's current in shared memory (64-bit fixed point, see
+// fx_add) and adds the tile into the global J in FP64.
 #include <cuda_runtime.h>
 #include <math.h>
 #include "pic_internal.cuh"
@@ -64,10 +64,13 @@ __device__ __forceinline__ float interp_mixed(const float *__restrict__ T, int S
     return t1 + t2;
 }
 
-// pqr (cell.h:1511-1693) in cell units: the segment xs -> xe (offsets relative
-// to the particle's cell origin) starting in the cell-centre index iv (2 or 3)
-__device__ __forceinline__ void pqr_mixed(float *__restrict__ sJ, int nn, int SY, int SZ, int n0, const int iv[3],
-                                          const float xs[3], const float xe[3], float wx, float wy, float wz) {
+// pqr (cell.h:1511-1693) in cell units: the 12 contributions of the segment
+// xs -> xe (offsets relative to the particle's cell origin) whose cell-centre
+// index is iv (2 or 3 per axis).  Order: Jx (0,0,0) (0,0,1) (0,1,0) (0,1,1),
+// Jy (0,0,0) (0,0,1) (1,0,0) (1,0,1), Jz (0,0,0) (0,1,0) (1,0,0) (1,1,0),
+// node offsets (x,y,z) relative to the base node iv.
+__device__ __forceinline__ void pqr_mixed(const int iv[3], const float xs[3], const float xe[3], float wx, float wy,
+                                          float wz, float v[12]) {
     float dx = 0.5f * (xs[0] + xe[0]) - ((float)iv[0] - 2.5f);
     float dy = 0.5f * (xs[1] + xe[1]) - ((float)iv[1] - 2.5f);
     float dz = 0.5f * (xs[2] + xe[2]) - ((float)iv[2] - 2.5f);
@@ -78,37 +81,121 @@ __device__ __forceinline__ void pqr_mixed(float *__restrict__ sJ, int nn, int SY
     su *= wx;
     sv *= wy;
     sw *= wz;
-    int n = n0 + (iv[0] * SY + iv[1]) * SZ + iv[2];
-    int ez = 1, ey = SZ, ex = SY * SZ;
-    float *Jx = sJ, *Jy = sJ + nn, *Jz = sJ + 2 * nn;
-    atomicAdd(&Jx[n], su * (dy1 * dz1 + s1));
-    atomicAdd(&Jx[n + ez], su * (dy1 * dz - s1));
-    atomicAdd(&Jx[n + ey], su * (dy * dz1 - s1));
-    atomicAdd(&Jx[n + ey + ez], su * (dy * dz + s1));
-    atomicAdd(&Jy[n], sv * (dx1 * dz1 + s2));
-    atomicAdd(&Jy[n + ez], sv * (dx1 * dz - s2));
-    atomicAdd(&Jy[n + ex], sv * (dx * dz1 - s2));
-    atomicAdd(&Jy[n + ex + ez], sv * (dx * dz + s2));
-    atomicAdd(&Jz[n], sw * (dx1 * dy1 + s3));
-    atomicAdd(&Jz[n + ey], sw * (dx1 * dy - s3));
-    atomicAdd(&Jz[n + ex], sw * (dx * dy1 - s3));
-    atomicAdd(&Jz[n + ex + ey], sw * (dx * dy + s3));
+    v[0] = su * (dy1 * dz1 + s1);
+    v[1] = su * (dy1 * dz - s1);
+    v[2] = su * (dy * dz1 - s1);
+    v[3] = su * (dy * dz + s1);
+    v[4] = sv * (dx1 * dz1 + s2);
+    v[5] = sv * (dx1 * dz - s2);
+    v[6] = sv * (dx * dz1 - s2);
+    v[7] = sv * (dx * dz + s2);
+    v[8] = sw * (dx1 * dy1 + s3);
+    v[9] = sw * (dx1 * dy - s3);
+    v[10] = sw * (dx * dy1 - s3);
+    v[11] = sw * (dx * dy + s3);
 }
 
+// tile-local J index of contribution j of a segment whose base node is nb
+__device__ __forceinline__ int contrib_node(int j, int nb, int nn, int SY, int SZ) {
+    int comp = j >> 2, r = j & 3;
+    int hi = r >> 1, lo = r & 1;
+    int dx = comp == 0 ? 0 : hi;
+    int dy = comp == 0 ? hi : (comp == 1 ? 0 : lo);
+    int dz = comp == 2 ? 0 : lo;
+    return comp * nn + nb + (dx * SY + dy) * SZ + dz;
+}
+
+// The split point of a segment that crosses cell-centre planes
+// (CurrentToMesh, cell.h:1338-1403), branch-free, in cell units.  An axis
+// whose centre index changes crosses the cell centre 1/2 and x2 lies on that
+// plane; the other coordinates follow the straight path at the parameter
+//   s = sum_c (1/2 - xs_c)(xe_c - xs_c) / sum_c (xe_c - xs_c)^2
+// over the crossing axes c -- the reference's formula for one crossing axis
+// (cases 1, 2, 4: a ratio) and for two (cases 3, 5, 6: the point nearest to
+// both planes); with three crossing axes x2 is the centre.  Without a crossing
+// x2 = xe: the second segment then has length 0 and adds nothing.
+__device__ __forceinline__ void split_point(const int i1[3], const int i2[3], const float xs[3], const float xe[3],
+                                            float x2[3]) {
+    float num = 0.f, den = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        float dl = xe[d] - xs[d];
+        bool c = i1[d] != i2[d];
+        num += c ? (0.5f - xs[d]) * dl : 0.f;
+        den += c ? dl * dl : 0.f;
+    }
+    const bool any = den > 0.f;
+    const float sr = any ? __fdividef(num, den) : 1.f;
+#pragma unroll
+    for (int d = 0; d < 3; d++) x2[d] = (i1[d] != i2[d]) ? 0.5f : xs[d] + (xe[d] - xs[d]) * sr;
+}
+
+// 2^e as float and double by exponent bits (no library call, no branch);
+// valid for -126 < e < 128
+__device__ __forceinline__ float pow2f(int e) { return __uint_as_float((unsigned)(e + 127) << 23); }
+__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+// e with 2^(e-1) <= x < 2^e for a positive normal float (0 for x = 0)
+__device__ __forceinline__ int exponent_above(float x) {
+    return x > 0.f ? (int)((__float_as_uint(x) >> 23) & 0xff) - 126 : 0;
+}
+
+// One particle's loaded state.
+struct PartM {
+    int cell;
+    float x, y, z, px, py, pz;
+};
+
+__device__ __forceinline__ PartM load_part(const SpeciesView &S, int slot) {
+    PartM p;
+    p.cell = S.cell[slot];
+    p.x = S.ox[slot]; p.y = S.oy[slot]; p.z = S.oz[slot];
+    p.px = S.fx[slot]; p.py = S.fy[slot]; p.pz = S.fz[slot];
+    return p;
+}
+
+// Deposit of the warp's current, two levels:
+//  1. lanes whose particle sits in the warp's lead cell add their contributions
+//     into a per-warp int32 scratch indexed by (cell-centre class, contribution)
+//     -- native 32-bit shared atomics, 96 words.  The warp's quantum q_w is a
+//     power of two above 64 x the largest possible contribution of any of its
+//     lanes (1.0834 |current of the full step|, reduced with redux.sync), so the
+//     int32 sums cannot overflow; rounding is below FP32 precision of that bound;
+//  2. the <= 96 distinct per-warp sums go into the tile's exact 64-bit
+//     fixed-point J (fx_add) -- no conflicts between lanes.
+// Lanes in other cells (unsorted bins) add straight into the tile J.
 __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int sNHoles, sNFront, sNMove;
     __shared__ double sRed[kPushThreads / 32];
+    __shared__ double sQ;
+    __shared__ int sTileE;
+    __shared__ float sInvQ;
+    __shared__ int sWarpAcc[kPushThreads / 32][96];
     const Grid &g = P.g;
     const int t = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
     const int tk = t % g.ntz, tl = (t / g.ntz) % g.nty, ti = t / (g.ntz * g.nty);
     const int i0 = ti * g.tx, l0 = tl * g.ty, k0 = tk * g.tz;
     const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
     const int nn = SX * SY * SZ;
-    float *sF = (float *)smem_raw;  // Ex Ey Ez Hx Hy Hz
-    float *sJ = sF + 6 * nn;
-    int *sHoles = (int *)(sJ + 3 * nn);
+    // fixed-point tile J first (8-byte aligned), then the FP32 field tile
+    unsigned long long *sJ = (unsigned long long *)smem_raw;
+    float *sF = (float *)(sJ + 3 * nn);  // Ex Ey Ez Hx Hy Hz
+    int *sHoles = (int *)(sF + 6 * nn);
     int *sFront = sHoles + kHoleMax;
+    int *wacc = sWarpAcc[warp];
+    if (threadIdx.x == 0) {
+        // quantum of the fixed-point tile J (see fx_add): |contribution| < 1.0834 |m| per segment
+        double bound = 0.0;
+        for (int s = 0; s < P.nsp; s++) bound += 2.5 * fabs(P.sp[s].m) * (double)P.sp[s].tile_count[t];
+        int e2;
+        frexp(bound, &e2);
+        sQ = ldexp(1.0, e2 - 62);
+        sTileE = e2 - 62;  // tile quantum 2^(e2-62)
+        sInvQ = (float)ldexp(1.0, 62 - e2);
+    }
+    for (int e = lane; e < 96; e += 32) wacc[e] = 0;
 
     const float *const *E = (const float *const *)P.E;
     const float *const *H = (const float *const *)P.H;
@@ -123,11 +210,13 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
         sF[3 * nn + idx] = in ? H[0][n] : 0.f;
         sF[4 * nn + idx] = in ? H[1][n] : 0.f;
         sF[5 * nn + idx] = in ? H[2][n] : 0.f;
-        sJ[idx] = 0.f;
-        sJ[nn + idx] = 0.f;
-        sJ[2 * nn + idx] = 0.f;
+        sJ[idx] = 0ull;
+        sJ[nn + idx] = 0ull;
+        sJ[2 * nn + idx] = 0ull;
     }
     __syncthreads();
+    const float inv_q = sInvQ;
+    const int tile_e = sTileE;
 
     const float ctx = (float)(g.tau / g.hx), cty = (float)(g.tau / g.hy), ctz = (float)(g.tau / g.hz);
     unsigned bad = 0;
@@ -145,19 +234,32 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
         const float wx = (float)(S.m * g.hx / g.tau), wy = (float)(S.m * g.hy / g.tau), wz = (float)(S.m * g.hz / g.tau);
         if (threadIdx.x == 0) { sNHoles = 0; sNFront = 0; sNMove = 0; }
         __syncthreads();
-        for (int j = threadIdx.x; j < count; j += blockDim.x) {
+        // warp-synchronous loop: every lane of a warp runs the same iterations;
+        // the next particle is loaded before the current one is processed
+        const int stride = blockDim.x;
+        PartM nxt;
+        nxt.cell = -1;
+        if (warp * 32 + lane < count) nxt = load_part(S, start + warp * 32 + lane);
+        for (int base = warp * 32; base < count; base += stride) {
+            const int j = base + lane;
             const int slot = start + j;
-            const int cell = S.cell[slot];
-            if (cell < 0) continue;
-            int k = cell % g.nz, l = (cell / g.nz) % g.ny, i = cell / (g.nz * g.ny);
-            if (i - i0 < 0 || i - i0 >= g.tx || l - l0 < 0 || l - l0 >= g.ty || k - k0 < 0 || k - k0 >= g.tz) {
-                bad |= ST_BADCELL;  // a bin entry outside its tile: never index the tile with it
-                continue;
+            PartM cur = nxt;
+            if (j + stride < count) nxt = load_part(S, slot + stride);
+            bool active = j < count && cur.cell >= 0;
+            int i = i0, l = l0, k = k0;
+            if (active) {
+                g.cell_ijk(cur.cell, i, l, k);
+                if (i - i0 < 0 || i - i0 >= g.tx || l - l0 < 0 || l - l0 >= g.ty || k - k0 < 0 || k - k0 >= g.tz) {
+                    bad |= ST_BADCELL;  // a bin entry outside its tile: never index the tile with it
+                    active = false;
+                    i = i0; l = l0; k = k0;
+                }
             }
             // tile-local node of reference tile index (0,0,0): cell_local - 2
             const int n0 = ((i - i0 - 2) * SY + (l - l0 - 2)) * SZ + (k - k0 - 2);
-            float xs[3] = {S.ox[slot], S.oy[slot], S.oz[slot]};
-            float pu = S.fx[slot], pv = S.fy[slot], pw = S.fz[slot];
+            float xs[3] = {cur.x, cur.y, cur.z};
+            if (!active) xs[0] = xs[1] = xs[2] = 0.25f;
+            float pu = active ? cur.px : 0.f, pv = active ? cur.py : 0.f, pw = active ? cur.pz : 0.f;
 
             // ---- GetField (cell.h:1257-1290) in cell units: getCellNumber = 2,
             // getCellNumberCenter = 2 + (offset >= 1/2), weights s1 = 1-o, s2 = 1/2-o (+1)
@@ -193,63 +295,84 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
             }
             float p2 = pu * pu + pv * pv + pw * pw;
             float ig = rsqrtf(p2 + 1.f);
-            if (!(isfinite(pu) && isfinite(pv) && isfinite(pw))) bad |= ST_NAN;
+            if (active && !(isfinite(pu) && isfinite(pv) && isfinite(pw))) bad |= ST_NAN;
             // gamma - 1 = p^2 / (gamma + 1), accumulated in FP64
-            kin += M * (double)(p2 / (1.f / ig + 1.f));
+            if (active) kin += M * (double)(p2 / (1.f / ig + 1.f));
             float xe[3] = {xs[0] + ctx * (ig * pu), xs[1] + cty * (ig * pv), xs[2] + ctz * (ig * pw)};
 
             // ---- CurrentToMesh (cell.h:1306-1422) in cell units
-            {
-                // cell-centre index of the end point from the same exact float
-                // thresholds as i1 (x + 2.5 rounded in FP32 would put a point one
-                // ulp below a centre plane on the far side of it)
-                int i1[3] = {i1x, i1y, i1z}, i2[3];
+            // cell-centre index of the end point from the same exact float
+            // thresholds as i1 (x + 2.5 rounded in FP32 would put a point one
+            // ulp below a centre plane on the far side of it)
+            const int i1[3] = {i1x, i1y, i1z};
+            int i2[3];
 #pragma unroll
-                for (int d = 0; d < 3; d++)
-                    i2[d] = 2 + (xe[d] >= 0.5f) + (xe[d] >= 1.5f) - (xe[d] < -0.5f);
-                if (i2[0] < 2 || i2[0] > 3 || i2[1] < 2 || i2[1] > 3 || i2[2] < 2 || i2[2] > 3) {
-                    bad |= ST_STENCIL;
-                } else {
-                    int m = 4 * abs(i2[0] - i1[0]) + 2 * abs(i2[1] - i1[1]) + abs(i2[2] - i1[2]);
-                    if (m == 0) {
-                        pqr_mixed(sJ, nn, SY, SZ, n0, i1, xs, xe, wx, wy, wz);
-                    } else {
-                        // the crossing plane of an axis that changes centre index is the cell centre 1/2
-                        float x2[3], sr;
-#define RATIO(d) ((x2[d] - xs[d]) / (xe[d] - xs[d]))
-#define PROD(d) ((x2[d] - xs[d]) * (xe[d] - xs[d]))
-#define SQ(v) ((v) * (v))
-#define RBX(d) (xs[d] + (xe[d] - xs[d]) * sr)
-                        switch (m) {
-                            case 1: x2[2] = 0.5f; sr = RATIO(2); x2[0] = RBX(0); x2[1] = RBX(1); break;
-                            case 2: x2[1] = 0.5f; sr = RATIO(1); x2[0] = RBX(0); x2[2] = RBX(2); break;
-                            case 3:
-                                x2[1] = 0.5f; x2[2] = 0.5f;
-                                sr = (PROD(2) + PROD(1)) / (SQ(xe[2] - xs[2]) + SQ(xe[1] - xs[1]));
-                                x2[0] = RBX(0);
-                                break;
-                            case 4: x2[0] = 0.5f; sr = RATIO(0); x2[1] = RBX(1); x2[2] = RBX(2); break;
-                            case 5:
-                                x2[0] = 0.5f; x2[2] = 0.5f;
-                                sr = (PROD(2) + PROD(0)) / (SQ(xe[2] - xs[2]) + SQ(xe[0] - xs[0]));
-                                x2[1] = RBX(1);
-                                break;
-                            case 6:
-                                x2[0] = 0.5f; x2[1] = 0.5f;
-                                sr = (PROD(1) + PROD(0)) / (SQ(xe[1] - xs[1]) + SQ(xe[0] - xs[0]));
-                                x2[2] = RBX(2);
-                                break;
-                            default: x2[0] = 0.5f; x2[1] = 0.5f; x2[2] = 0.5f; break;
+            for (int d = 0; d < 3; d++) i2[d] = 2 + (xe[d] >= 0.5f) + (xe[d] >= 1.5f) - (xe[d] < -0.5f);
+            bool dep = active && isfinite(xe[0]) && isfinite(xe[1]) && isfinite(xe[2]);
+            if (dep && (i2[0] < 2 || i2[0] > 3 || i2[1] < 2 || i2[1] > 3 || i2[2] < 2 || i2[2] > 3)) {
+                bad |= ST_STENCIL;
+                dep = false;
+            }
+            // warp quantum: 2^(ew-22) with 2^(ew-1) <= wmax < 2^ew, wmax the largest
+            // contribution bound of the warp's lanes (1.0834 |current of the full
+            // step|, redux.sync max).  Contributions then scale to |w| < 2^22, so the
+            // FMA magic-number rounding below is exact, and 64 of them sum below 2^28.
+            const float lb = dep ? 1.0834f * fmaxf(fabsf(wx * (xe[0] - xs[0])),
+                                                   fmaxf(fabsf(wy * (xe[1] - xs[1])), fabsf(wz * (xe[2] - xs[2]))))
+                                 : 0.f;
+            const float wmax = __uint_as_float(__reduce_max_sync(FULL, __float_as_uint(lb)));
+            const int ew = max(exponent_above(wmax), -100);
+            const float inv_qw = pow2f(22 - ew);
+            const int sh = ew - 22 - tile_e;  // warp quantum / tile quantum = 2^sh
+            const unsigned am = __ballot_sync(FULL, dep);
+            const int lead = am ? __ffs(am) - 1 : 0;
+            const int lead_cell = __shfl_sync(FULL, cur.cell, lead);
+            const bool fast = dep && cur.cell == lead_cell;
+            if (dep) {
+                // two segments for every lane; the second has length 0 without a crossing
+                float x2[3], v[12];
+                split_point(i1, i2, xs, xe, x2);
+                auto deposit = [&](const int iv[3]) {
+                    const int cls = ((iv[0] - 2) << 2) | ((iv[1] - 2) << 1) | (iv[2] - 2);
+                    if (fast) {
+#pragma unroll
+                        for (int q = 0; q < 12; q++) {
+                            int w = __float_as_int(fmaf(v[q], inv_qw, 12582912.0f)) - 0x4B400000;  // round(v/q_w)
+                            if (w) atomicAdd(&wacc[cls * 12 + q], w);
                         }
-#undef RATIO
-#undef PROD
-#undef SQ
-#undef RBX
-                        pqr_mixed(sJ, nn, SY, SZ, n0, i1, xs, x2, wx, wy, wz);
-                        pqr_mixed(sJ, nn, SY, SZ, n0, i2, x2, xe, wx, wy, wz);
+                    } else {
+                        const int nb = n0 + (iv[0] * SY + iv[1]) * SZ + iv[2];
+#pragma unroll
+                        for (int q = 0; q < 12; q++) fx_addf(&sJ[contrib_node(q, nb, nn, SY, SZ)], v[q], inv_q);
+                    }
+                };
+                pqr_mixed(i1, xs, x2, wx, wy, wz, v);
+                deposit(i1);
+                pqr_mixed(i2, x2, xe, wx, wy, wz, v);
+                deposit(i2);
+            }
+            __syncwarp();
+            if (am) {
+                // flush the per-warp sums of the lead cell into the tile J (exact: both
+                // quanta are powers of two, the tile bound keeps the result below 2^62)
+                int li, ll, lk;
+                g.cell_ijk(lead_cell, li, ll, lk);
+                const int ln0 = ((li - i0 - 2) * SY + (ll - l0 - 2)) * SZ + (lk - k0 - 2);
+                for (int e = lane; e < 96; e += 32) {
+                    int w = wacc[e];
+                    if (w) {
+                        wacc[e] = 0;
+                        int cls = e / 12, q = e - cls * 12;
+                        int nb = ln0 + ((2 + (cls >> 2)) * SY + (2 + ((cls >> 1) & 1))) * SZ + 2 + (cls & 1);
+                        long long add = sh >= 0 ? (long long)w << sh
+                                        : (sh > -62 ? ((long long)w + (1ll << (-sh - 1))) >> (-sh) : 0ll);
+                        if (add) atomicAdd(&sJ[contrib_node(q, nb, nn, SY, SZ)], (unsigned long long)add);
                     }
                 }
             }
+            __syncwarp();
+
+            if (!active) continue;
             // ---- new cell (Reflect cell.h:1427-1478 and migration, in cell units)
             int ci[3] = {i, l, k};
             const int nc[3] = {g.nx, g.ny, g.nz};
@@ -265,7 +388,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
                 xe[d] = fminf(fmaxf(xe[d], 0.f), kOneBelow);
             }
             const int newcell = g.cell_of(ci[0], ci[1], ci[2]);
-            if (newcell == cell || g.tile_of_cell(ci[0], ci[1], ci[2]) == t) {
+            if (newcell == cur.cell || g.tile_of_cell(ci[0], ci[1], ci[2]) == t) {
                 S.cell[slot] = newcell;
                 S.ox[slot] = xe[0]; S.oy[slot] = xe[1]; S.oz[slot] = xe[2];
                 S.fx[slot] = pu; S.fy[slot] = pv; S.fz[slot] = pw;
@@ -299,9 +422,9 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
             for (int r = threadIdx.x; r < L; r += blockDim.x) {
                 int src = start + newcount + r;
                 if (S.cell[src] >= 0) {
-                    int m = atomicAdd(&sNMove, 1);
-                    if (m >= sNFront) { bad |= ST_BADCELL; continue; }
-                    int dst = start + sFront[m];
+                    int mv = atomicAdd(&sNMove, 1);
+                    if (mv >= sNFront) { bad |= ST_BADCELL; continue; }
+                    int dst = start + sFront[mv];
                     S.cell[dst] = S.cell[src];
                     S.ox[dst] = S.ox[src]; S.oy[dst] = S.oy[src]; S.oz[dst] = S.oz[src];
                     S.fx[dst] = S.fx[src]; S.fy[dst] = S.fy[src]; S.fz[dst] = S.fz[src];
@@ -313,12 +436,12 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     }
 
     for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
-        float v = sJ[idx];
-        if (v != 0.f) {
+        long long iv = (long long)sJ[idx];
+        if (iv != 0) {
             int comp = idx / nn, r = idx % nn;
             int c = r % SZ, b = (r / SZ) % SY, a = r / (SZ * SY);
             if (i0 + a < g.NX && l0 + b < g.NY && k0 + c < g.NZ)
-                atomicAdd(&P.J[comp][g.node(i0 + a, l0 + b, k0 + c)], (double)v);
+                atomicAdd(&P.J[comp][g.node(i0 + a, l0 + b, k0 + c)], (double)iv * sQ);
         }
     }
     for (int o = 16; o > 0; o >>= 1) kin += __shfl_down_sync(0xffffffffu, kin, o);
@@ -352,7 +475,7 @@ void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], dou
 
 size_t push_smem_mixed(const Grid &g) {
     size_t nn = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2);
-    return 9 * nn * sizeof(float) + 2 * kHoleMax * sizeof(int);
+    return 6 * nn * sizeof(float) + 3 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
 }
 
 cudaError_t launch_push_mixed(const StepParams &p, cudaStream_t s) {

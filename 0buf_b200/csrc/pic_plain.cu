@@ -166,10 +166,10 @@ __device__ __forceinline__ double interp_plain(const double *__restrict__ T, int
 }
 
 // pqr, cell.h:1511-1693, accumulating into the tile J (shared memory)
-__device__ __forceinline__ void pqr_plain(double *__restrict__ sJ, int nn, int SY, int SZ, int bi, int bl, int bk,
-                                          const int iv[3], const double x[3], const double x1[3], double a1,
-                                          double hx, double hy, double hz, double tau, double x0, double y0,
-                                          double z0, unsigned &bad) {
+__device__ __forceinline__ void pqr_plain(unsigned long long *__restrict__ sJ, double inv_q, int nn, int SY, int SZ,
+                                          int bi, int bl, int bk, const int iv[3], const double x[3],
+                                          const double x1[3], double a1, double hx, double hy, double hz, double tau,
+                                          double x0, double y0, double z0, unsigned &bad) {
     double dx = (0.50 * (x[0] + x1[0]) - hx * ((double)iv[0] - 2.50) - x0);
     double dy = (0.50 * (x[1] + x1[1]) - hy * ((double)iv[1] - 2.50) - y0);
     double dz = (0.50 * (x[2] + x1[2]) - hz * ((double)iv[2] - 2.50) - z0);
@@ -183,19 +183,19 @@ __device__ __forceinline__ void pqr_plain(double *__restrict__ sJ, int nn, int S
     if (iv[0] < 2 || iv[0] > 3 || iv[1] < 2 || iv[1] > 3 || iv[2] < 2 || iv[2] > 3) { bad |= ST_STENCIL; return; }
     int n = ((bi + iv[0]) * SY + (bl + iv[1])) * SZ + (bk + iv[2]);
     int ez = 1, ey = SZ, ex = SY * SZ;
-    double *Jx = sJ, *Jy = sJ + nn, *Jz = sJ + 2 * nn;
-    atomicAdd(&Jx[n], su * (dy1 * dz1 + s1));
-    atomicAdd(&Jx[n + ez], su * (dy1 * dz - s1));
-    atomicAdd(&Jx[n + ey], su * (dy * dz1 - s1));
-    atomicAdd(&Jx[n + ey + ez], su * (dy * dz + s1));
-    atomicAdd(&Jy[n], sv * (dx1 * dz1 + s2));
-    atomicAdd(&Jy[n + ez], sv * (dx1 * dz - s2));
-    atomicAdd(&Jy[n + ex], sv * (dx * dz1 - s2));
-    atomicAdd(&Jy[n + ex + ez], sv * (dx * dz + s2));
-    atomicAdd(&Jz[n], sw * (dx1 * dy1 + s3));
-    atomicAdd(&Jz[n + ey], sw * (dx1 * dy - s3));
-    atomicAdd(&Jz[n + ex], sw * (dx * dy1 - s3));
-    atomicAdd(&Jz[n + ex + ey], sw * (dx * dy + s3));
+    unsigned long long *Jx = sJ, *Jy = sJ + nn, *Jz = sJ + 2 * nn;
+    fx_add(&Jx[n], su * (dy1 * dz1 + s1), inv_q);
+    fx_add(&Jx[n + ez], su * (dy1 * dz - s1), inv_q);
+    fx_add(&Jx[n + ey], su * (dy * dz1 - s1), inv_q);
+    fx_add(&Jx[n + ey + ez], su * (dy * dz + s1), inv_q);
+    fx_add(&Jy[n], sv * (dx1 * dz1 + s2), inv_q);
+    fx_add(&Jy[n + ez], sv * (dx1 * dz - s2), inv_q);
+    fx_add(&Jy[n + ex], sv * (dx * dz1 - s2), inv_q);
+    fx_add(&Jy[n + ex + ez], sv * (dx * dz + s2), inv_q);
+    fx_add(&Jz[n], sw * (dx1 * dy1 + s3), inv_q);
+    fx_add(&Jz[n + ey], sw * (dx1 * dy - s3), inv_q);
+    fx_add(&Jz[n + ex], sw * (dx * dy1 - s3), inv_q);
+    fx_add(&Jz[n + ex + ey], sw * (dx * dy + s3), inv_q);
 }
 
 // Reflect, cell.h:1427-1478
@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int sNHoles, sNFront, sNMove;
     __shared__ double sRed[kPushThreads / 32];
+    __shared__ double sQ, sInvQ;
     const Grid &g = P.g;
     const int t = blockIdx.x;
     const int tk = t % g.ntz, tl = (t / g.ntz) % g.nty, ti = t / (g.ntz * g.nty);
@@ -229,9 +230,17 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
     const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
     const int nn = SX * SY * SZ;
     double *sF = (double *)smem_raw;  // Ex Ey Ez Hx Hy Hz
-    double *sJ = sF + 6 * nn;
+    unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);  // fixed-point tile J
     int *sHoles = (int *)(sJ + 3 * nn);
     int *sFront = sHoles + kHoleMax;
+    if (threadIdx.x == 0) {
+        double bound = 0.0;
+        for (int s = 0; s < P.nsp; s++) bound += 2.5 * fabs(P.sp[s].m) * (double)P.sp[s].tile_count[t];
+        int e2;
+        frexp(bound, &e2);  // bound < 2^e2
+        sQ = ldexp(1.0, e2 - 62);
+        sInvQ = ldexp(1.0, 62 - e2);
+    }
 
     // stage E^n and H^{n+1/2} of nodes [i0, i0+tx+2) x [l0, ..) x [k0, ..)
     // (GPU_SetFieldsToCells, kernels.cu:32-49, for all cells of the tile at once)
@@ -248,13 +257,14 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
         sF[3 * nn + idx] = in ? H[0][n] : 0.0;
         sF[4 * nn + idx] = in ? H[1][n] : 0.0;
         sF[5 * nn + idx] = in ? H[2][n] : 0.0;
-        sJ[idx] = 0.0;
-        sJ[nn + idx] = 0.0;
-        sJ[2 * nn + idx] = 0.0;
+        sJ[idx] = 0ull;
+        sJ[nn + idx] = 0ull;
+        sJ[2 * nn + idx] = 0ull;
     }
     __syncthreads();
 
     const double hx = g.hx, hy = g.hy, hz = g.hz, tau = g.tau;
+    const double inv_q = sInvQ;
     unsigned bad = 0;
     double kin = 0.0;
     unsigned long long moved = 0, dropped = 0, dup = 0;
@@ -271,7 +281,8 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
             const int slot = start + j;
             const int cell = S.cell[slot];
             if (cell < 0) continue;  // dead slot left by an overflowed compaction
-            const int k = cell % g.nz, l = (cell / g.nz) % g.ny, i = cell / (g.nz * g.ny);
+            int i, l, k;
+            g.cell_ijk(cell, i, l, k);
             const int bi = i - i0 - 2, bl = l - l0 - 2, bk = k - k0 - 2;
             if (bi < -2 || bi >= g.tx - 2 || bl < -2 || bl >= g.ty - 2 || bk < -2 || bk >= g.tz - 2) {
                 bad |= ST_BADCELL;  // a bin entry outside its tile: never index the tile with it
@@ -381,10 +392,10 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
 #undef RBX
 #undef SQ
                 if (m >= 1 && m <= 7) {
-                    pqr_plain(sJ, nn, SY, SZ, bi, bl, bk, i1, xo, x2, mw, hx, hy, hz, tau, x0, y0, z0, bad);
-                    pqr_plain(sJ, nn, SY, SZ, bi, bl, bk, i2, x2, xn, mw, hx, hy, hz, tau, x0, y0, z0, bad);
+                    pqr_plain(sJ, inv_q, nn, SY, SZ, bi, bl, bk, i1, xo, x2, mw, hx, hy, hz, tau, x0, y0, z0, bad);
+                    pqr_plain(sJ, inv_q, nn, SY, SZ, bi, bl, bk, i2, x2, xn, mw, hx, hy, hz, tau, x0, y0, z0, bad);
                 } else {
-                    pqr_plain(sJ, nn, SY, SZ, bi, bl, bk, i1, xo, xn, mw, hx, hy, hz, tau, x0, y0, z0, bad);
+                    pqr_plain(sJ, inv_q, nn, SY, SZ, bi, bl, bk, i1, xo, xn, mw, hx, hy, hz, tau, x0, y0, z0, bad);
                 }
             }
             x = reflect_plain(xn[0], g.lx);
@@ -470,12 +481,12 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
 
     // ---- tile J -> global J (GPU_WriteAllCurrents, kernels.cu:83-112)
     for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
-        double v = sJ[idx];
-        if (v != 0.0) {
+        long long iv = (long long)sJ[idx];
+        if (iv != 0) {
             int comp = idx / nn, r = idx % nn;
             int c = r % SZ, b = (r / SZ) % SY, a = r / (SZ * SY);
             if (i0 + a < g.NX && l0 + b < g.NY && k0 + c < g.NZ)
-                atomicAdd(&P.J[comp][g.node(i0 + a, l0 + b, k0 + c)], v);
+                atomicAdd(&P.J[comp][g.node(i0 + a, l0 + b, k0 + c)], (double)iv * sQ);
         }
     }
     // ---- kinetic energy and counters
@@ -563,7 +574,7 @@ void e_ghosts_mixed(const Grid &g, float *Ex, float *Ey, float *Ez, int periodic
 
 size_t push_smem_plain(const Grid &g) {
     size_t nn = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2);
-    return 9 * nn * sizeof(double) + 2 * kHoleMax * sizeof(int);
+    return 6 * nn * sizeof(double) + 3 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
 }
 
 cudaError_t launch_push_plain(const StepParams &p, cudaStream_t s) {
