@@ -41,9 +41,12 @@ UNIT = "particle-steps/s"
 BYTES_PER_PARTICLE_STEP = {"fp32": 56, "fp64": 104}
 # algorithmic bytes per Yee cell-update: read E, B, J and write E, B
 BYTES_PER_CELL_UPDATE = {"fp32": 72, "fp64": 120}
-# DRAM bytes per particle of the push kernel from one ncu capture
-# (profiles/push_mixed_c2_ncu.md); None until measured
-NCU_TRAFFIC_PER_PARTICLE = {"fp32": None, "fp64": None}
+# DRAM bytes per particle of the push kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture of 50,331,648 particles, scaled to
+# a launch by particle count since the kernel's traffic is proportional to it):
+# profiles/push_mixed_128x64x64_ncu.md (2.820 GB) and
+# profiles/push_plain_128x64x64_ncu.md (5.271 GB)
+NCU_TRAFFIC_PER_PARTICLE = {"fp32": 2.820e9 / 50331648, "fp64": 5.271e9 / 50331648}
 KERNELS_PER_STEP_NOTE = "b_half, push, insert, clamp, j_fold x3, b_complete, e_update, e_ghosts x2"
 
 
