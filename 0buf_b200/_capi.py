@@ -91,6 +91,7 @@ SIGNATURES = {
     "pic_step_timings": (C.c_int, [H, F]),
     "pic_layout_info": (C.c_int, [H, I64]),
     "pic_stream": (C.c_void_p, [H]),
+    "pic_field_energy_noalloc": (C.c_int, [C.c_int] * 3 + [C.c_void_p] * 8),
     # archAPI replacement (pic0buf_arch.h)
     "MemoryCopy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]),
     "MemoryAllocate": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),

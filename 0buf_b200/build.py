@@ -34,6 +34,7 @@ UNITS = {
     "pic_capi.cu": ["-fmad=false"],
     "pic_arch.cu": [],
     "pic_mixed.cu": [],
+    "pic_noalloc.cu": [],
 }
 
 

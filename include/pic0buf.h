@@ -180,6 +180,27 @@ int pic_energy_reference(pic_handle *h, double *out);
  * style check -- see pic_charge_residual in the implementation notes. */
 int pic_charge_density(pic_handle *h, double *rho_host);
 
+/* Field energies without any allocation.  No counterpart in the reference.
+ * For callers that cannot let the library call cudaMalloc (their framework
+ * owns all device memory, or a timed loop cannot take cudaMalloc's implicit
+ * device synchronisation).  Inputs: caller-owned DEVICE arrays of one field
+ * component each in the reference layout ((Nx+2)(Ny+2)(Nz+2) FP64).  Output:
+ * out3 (DEVICE, 3 doubles) = 1/2 sum E^2 and 1/2 sum H^2 over the nodes 1..N
+ * of every axis (as pic_energy), and sum E^2 over all nodes (as
+ * pic_energy_reference).  Work is enqueued on `stream` (a cudaStream_t, NULL
+ * for the default stream); the result is ready when the stream reaches it.
+ * Scratch: a file-scope device array of PIC_NOALLOC_MAX_BLOCKS x 3 doubles
+ * (1.5 MB) that every GPU loading the library holds until exit; at most
+ * PIC_NOALLOC_MAX_NODES nodes, larger grids return PIC_ERR_ARG.  The first
+ * call on a device looks the array's device address up (cudaGetSymbolAddress),
+ * so make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race;
+ * serialise them.  The result is deterministic (fixed-order sums). */
+#define PIC_NOALLOC_MAX_BLOCKS 65536
+#define PIC_NOALLOC_MAX_NODES (PIC_NOALLOC_MAX_BLOCKS * 256)
+int pic_field_energy_noalloc(int nx, int ny, int nz, const double *Ex, const double *Ey, const double *Ez,
+                             const double *Hx, const double *Hy, const double *Hz, double *out3, void *stream);
+
 /* Status and errors. */
 int pic_sync(pic_handle *h);
 int pic_last_status(pic_handle *h);
