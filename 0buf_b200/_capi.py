@@ -46,6 +46,16 @@ class PicConfig(C.Structure):
     ]
 
 
+class PicLoss(C.Structure):
+    _fields_ = [("field", C.c_int), ("window", C.c_int), ("species", C.c_int), ("reserved_i", C.c_int),
+                ("drift", C.c_double * 3), ("vth", C.c_double), ("reserved", C.c_double * 4)]
+
+
+class PicGrads(C.Structure):
+    _fields_ = [("loss", C.c_double), ("d_drift", C.c_double * 3), ("d_vth", C.c_double), ("n", C.c_int64),
+                ("d_p0", C.c_void_p), ("reserved", C.c_double * 4)]
+
+
 D = C.POINTER(C.c_double)
 F = C.POINTER(C.c_float)
 I32 = C.POINTER(C.c_int)
@@ -91,6 +101,12 @@ SIGNATURES = {
     "pic_step_timings": (C.c_int, [H, F]),
     "pic_layout_info": (C.c_int, [H, I64]),
     "pic_stream": (C.c_void_p, [H]),
+    "pic_forward": (C.c_int, [H, C.c_int, C.c_int]),
+    "pic_forward_history": (C.c_int, [H, D]),
+    "pic_loss_value": (C.c_int, [H, C.POINTER(PicLoss), D]),
+    "pic_backward": (C.c_int, [H, C.POINTER(PicLoss), C.POINTER(PicGrads)]),
+    "pic_adjoint_timings": (C.c_int, [H, F]),
+    "pic_adjoint_free": (C.c_int, [H]),
     "pic_field_energy_noalloc": (C.c_int, [C.c_int] * 3 + [C.c_void_p] * 8),
     # archAPI replacement (pic0buf_arch.h)
     "MemoryCopy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]),

@@ -35,6 +35,8 @@ UNITS = {
     "pic_arch.cu": [],
     "pic_mixed.cu": [],
     "pic_noalloc.cu": [],
+    "pic_adjoint.cu": ["-fmad=false"],
+    "pic_adjoint_mixed.cu": [],
 }
 
 

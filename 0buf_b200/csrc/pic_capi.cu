@@ -15,42 +15,12 @@
 #include "pic_internal.cuh"
 #include "pic_kernels.cuh"
 #include "pic_rng.cuh"
+#include "pic_handle.cuh"
 
 using namespace pic;
+using namespace pic_host;
 
-struct pic_handle {
-    pic_config cfg;
-    Grid g;
-    int mixed;
-    int device;
-    cudaStream_t stream;
-    void *f[PIC_FIELD_COUNT];  // plain: 12 double arrays; mixed: E,H float, J double, Q null
-    double *dense;             // one reference-layout FP64 array (I/O staging)
-    struct Sp {
-        SpeciesView v;
-        int64_t cap_total;
-        int loaded;
-        std::vector<int> h_start;
-    } sp[kMaxSpecies];
-    void *outbox;
-    unsigned out_cap;
-    size_t out_elem;
-    DevStatus *st;
-    DevStatus *st_host;
-    double *dred;   // device reduction scratch
-    double *hred;   // pinned
-    int *dcounts;   // ncells ints
-    int status;
-    char err[256];
-    int64_t counters[4];
-    float timings[5];
-    cudaEvent_t ev[6];
-    int64_t launches;  // kernels launched by the current/last step
-    int timed;
-    int kin_valid;  // st->kinetic holds the kinetic energy of the current momenta
-};
-
-namespace {
+namespace pic_host {
 
 int set_err(pic_handle *h, int code, const char *msg) {
     if (h) {
@@ -68,11 +38,6 @@ int cuda_err(pic_handle *h, cudaError_t e, const char *where) {
     return set_err(h, (int)e, buf);
 }
 
-#define CK(expr, where)                                   \
-    do {                                                  \
-        cudaError_t e_ = (expr);                          \
-        if (e_ != cudaSuccess) return cuda_err(h, e_, where); \
-    } while (0)
 
 size_t elem_particle(int mixed) { return mixed ? 28 : 52; }
 
@@ -196,6 +161,25 @@ int build_bins(pic_handle *h, int s, int64_t n, int *cell, const double *x, cons
     return build_bins_with(h, s, n, cell, [&](const SpeciesView &v, int *fill) {
         return scatter_to_bins(g, mixed, n, cell, x, y, z, px, py, pz, v, fill, st);
     }, inserted);
+}
+
+int build_bins_f(pic_handle *h, int s, int64_t n, int *cell, const float *ox, const float *oy, const float *oz,
+                 const float *px, const float *py, const float *pz) {
+    const Grid &g = h->g;
+    int mixed = h->mixed;
+    cudaStream_t st = h->stream;
+    return build_bins_with(h, s, n, cell, [&](const SpeciesView &v, int *fill) {
+        return scatter_to_bins_f(g, mixed, n, cell, ox, oy, oz, px, py, pz, v, fill, st);
+    }, nullptr);
+}
+
+int tile_counts(pic_handle *h, int s, std::vector<int> &counts) {
+    counts.assign(h->g.ntiles, 0);
+    if (!h->sp[s].loaded) return PIC_OK;
+    CK(cudaMemcpyAsync(counts.data(), h->sp[s].v.tile_count, h->g.ntiles * sizeof(int), cudaMemcpyDeviceToHost,
+                       h->stream), "counts");
+    CK(cudaStreamSynchronize(h->stream), "sync");
+    return PIC_OK;
 }
 
 int load_device(pic_handle *h, int s, int64_t n, const double *x, const double *y, const double *z,
@@ -371,7 +355,7 @@ int set_device(pic_handle *h) {
     return PIC_OK;
 }
 
-}  // namespace
+}  // namespace pic_host
 
 extern "C" {
 
@@ -481,6 +465,7 @@ int pic_destroy(pic_handle *h) {
     if (!h) return PIC_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    adj_free(h);
     for (int s = 0; s < h->cfg.nspecies; s++) free_species(h, s);
     for (int fi = 0; fi < PIC_FIELD_COUNT; fi++)
         if (h->f[fi]) cudaFree(h->f[fi]);

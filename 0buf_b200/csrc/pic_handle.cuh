@@ -1,0 +1,73 @@
+// The handle behind the C ABI (pic_handle) and the host helpers shared by the
+// translation units that implement the ABI (pic_capi.cu: the step and I/O;
+// pic_adjoint.cu: the differentiable run).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <vector>
+#include "pic0buf.h"
+#include "pic_internal.cuh"
+
+namespace pic {
+struct AdjState;  // checkpoints and adjoint buffers of the differentiable run (pic_adjoint.cu)
+}
+
+struct pic_handle {
+    pic_config cfg;
+    pic::Grid g;
+    int mixed;
+    int device;
+    cudaStream_t stream;
+    void *f[PIC_FIELD_COUNT];  // plain: 12 double arrays; mixed: E,H float, J double, Q null
+    double *dense;             // one reference-layout FP64 array (I/O staging)
+    struct Sp {
+        pic::SpeciesView v;
+        int64_t cap_total;
+        int loaded;
+        std::vector<int> h_start;
+    } sp[pic::kMaxSpecies];
+    void *outbox;
+    unsigned out_cap;
+    size_t out_elem;
+    pic::DevStatus *st;
+    pic::DevStatus *st_host;
+    double *dred;   // device reduction scratch
+    double *hred;   // pinned
+    int *dcounts;   // ncells ints
+    int status;
+    char err[256];
+    int64_t counters[4];
+    float timings[5];
+    cudaEvent_t ev[6];
+    int64_t launches;  // kernels launched by the current/last step
+    int timed;
+    int kin_valid;  // st->kinetic holds the kinetic energy of the current momenta
+    pic::AdjState *adj;
+};
+
+namespace pic_host {
+
+int set_err(pic_handle *h, int code, const char *msg);
+int cuda_err(pic_handle *h, cudaError_t e, const char *where);
+int set_device(pic_handle *h);
+int need_particles(pic_handle *h);
+// flat device list of one species (packed cell, FP64 global positions and
+// momenta; cell < 0 = rejected) -> bins of species s
+int build_bins(pic_handle *h, int s, int64_t n, int *cell, const double *x, const double *y, const double *z,
+               const double *px, const double *py, const double *pz, int64_t *inserted);
+// flat device list in the native layout (packed cell, FP32 offsets and momenta) -> bins of species s
+int build_bins_f(pic_handle *h, int s, int64_t n, int *cell, const float *ox, const float *oy, const float *oz,
+                 const float *px, const float *py, const float *pz);
+// live particles per tile of species s (host copy)
+int tile_counts(pic_handle *h, int s, std::vector<int> &counts);
+// the differentiable run's buffers (pic_adjoint.cu)
+void adj_free(pic_handle *h);
+
+}  // namespace pic_host
+
+#define CK(expr, where)                                                    \
+    do {                                                                   \
+        cudaError_t e_ = (expr);                                           \
+        if (e_ != cudaSuccess) return pic_host::cuda_err(h, e_, where);    \
+    } while (0)

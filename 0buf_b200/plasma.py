@@ -195,6 +195,62 @@ class PicSimulation:
         self._ck(self.lib.pic_layout_info(self.h, v.ctypes.data_as(_capi.I64)), "pic_layout_info")
         return dict(tiles=int(v[0]), slots=int(v[1]), bytes_per_particle=int(v[2]), nodes=int(v[3]))
 
+    # ------------------------------------------------- differentiable run
+    def forward(self, steps: int, ckpt_every: int):
+        """``pic_forward``: advance ``steps`` steps, checkpointing every ``ckpt_every``."""
+        self._ck(self.lib.pic_forward(self.h, int(steps), int(ckpt_every)), "pic_forward")
+        self._fwd_steps = int(steps)
+
+    def history(self) -> np.ndarray:
+        """(steps, 3): h^3 * sum over nodes 1..N of E_c^2 after each step of the last forward run."""
+        out = np.zeros((self._fwd_steps, 3))
+        self._ck(self.lib.pic_forward_history(self.h, dptr(out)), "pic_forward_history")
+        return out
+
+    @staticmethod
+    def make_loss(field: str = "Ex", window: int = 1, species: int = 0, drift=(0.0, 0.0, 0.0),
+                  vth: float = 0.0) -> _capi.PicLoss:
+        L = _capi.PicLoss()
+        L.field = {"Ex": 0, "Ey": 1, "Ez": 2}[field]
+        L.window = int(window)
+        L.species = int(species)
+        for a in range(3):
+            L.drift[a] = float(drift[a])
+        L.vth = float(vth)
+        return L
+
+    def loss_value(self, **loss) -> float:
+        v = np.zeros(1)
+        L = self.make_loss(**loss)
+        self._ck(self.lib.pic_loss_value(self.h, C.byref(L), dptr(v)), "pic_loss_value")
+        return float(v[0])
+
+    def backward(self, want_p0: bool = True, **loss) -> dict:
+        """``pic_backward``: loss value, dL/d drift, dL/d vth and dL/dp0 (n, 3) of ``species``,
+        in ``particles(species)`` order as of the call to ``forward``."""
+        L = self.make_loss(**loss)
+        G = _capi.PicGrads()
+        buf = None
+        if want_p0:
+            n = self.num_particles(L.species)  # the differentiable run keeps every particle
+            buf = np.zeros((max(n, 1), 3))
+            G.n = n
+            G.d_p0 = buf.ctypes.data
+        self._ck(self.lib.pic_backward(self.h, C.byref(L), C.byref(G)), "pic_backward")
+        out = dict(loss=G.loss, d_drift=np.array(G.d_drift[:]), d_vth=G.d_vth, n=int(G.n))
+        if buf is not None:
+            out["d_p0"] = buf[:G.n]
+        return out
+
+    def adjoint_timings(self) -> np.ndarray:
+        """[forward, backward] device milliseconds of the last differentiable run."""
+        t = np.zeros(2, np.float32)
+        self._ck(self.lib.pic_adjoint_timings(self.h, t.ctypes.data_as(_capi.F)), "pic_adjoint_timings")
+        return t
+
+    def adjoint_free(self):
+        self._ck(self.lib.pic_adjoint_free(self.h), "pic_adjoint_free")
+
 
 def _host_ptr(a):
     if isinstance(a, np.ndarray):

@@ -180,6 +180,52 @@ int pic_energy_reference(pic_handle *h, double *out);
  * style check -- see pic_charge_residual in the implementation notes. */
 int pic_charge_density(pic_handle *h, double *rho_host);
 
+/* Differentiable run (no counterpart in the reference, which has no
+ * gradients).  pic_forward advances the state by `steps` time steps with the
+ * same physics as pic_step, keeping every particle in a fixed order, stores
+ * the particles and E/B every `ckpt_every` steps, and records the history
+ * W[n][c] = h_x h_y h_z sum over nodes 1..N of E_c^2 after step n.
+ * pic_backward then sweeps the steps in reverse -- per checkpoint segment it
+ * recomputes the forward states and runs the adjoint kernels (transpose of
+ * the ghost copies, the E update, the J fold and the B half steps; the
+ * deposit's transpose as a gather; the push Jacobian with the interpolation's
+ * transpose as a scatter) -- and returns the gradient of
+ *   L = sum over the last `window` steps n of W[n][field]
+ * with respect to the initial momenta of one species, and through
+ * p0 = drift + vth * xi to that species' drift and thermal spread.
+ * Particle order of the gradient = pic_get_particles order at the call to
+ * pic_forward.  The buffers stay allocated until pic_adjoint_free, the next
+ * pic_forward or pic_destroy.  Both forms are supported: the plain form
+ * differentiates in FP64, the mixed form in FP32 (particles) with FP64 field
+ * adjoints. */
+typedef struct pic_loss {
+    int field;        /* PIC_EX, PIC_EY or PIC_EZ */
+    int window;       /* last steps of the forward run that the loss sums, 1..steps */
+    int species;      /* species of the momentum gradient */
+    int reserved_i;
+    double drift[3];  /* that species' drift at initialisation */
+    double vth;       /* that species' thermal spread at initialisation (> 0 for d_vth) */
+    double reserved[4];
+} pic_loss;
+
+typedef struct pic_grads {
+    double loss;        /* out: L */
+    double d_drift[3];  /* out: dL/d drift */
+    double d_vth;       /* out: dL/d vth = sum_i dL/dp_i . (p_i - drift)/vth */
+    int64_t n;          /* in: capacity of d_p0 in particles; out: particles of the species */
+    double *d_p0;       /* in: host array of 3*n doubles (px, py, pz of each particle) or NULL */
+    double reserved[4];
+} pic_grads;
+
+int pic_forward(pic_handle *h, int steps, int ckpt_every);
+/* out[n*3 + c] = W[n][c] of the last forward run (host array of 3*steps) */
+int pic_forward_history(pic_handle *h, double *out);
+int pic_loss_value(pic_handle *h, const pic_loss *loss, double *value);
+int pic_backward(pic_handle *h, const pic_loss *loss, pic_grads *grads);
+/* device time of the last pic_forward and pic_backward, milliseconds */
+int pic_adjoint_timings(pic_handle *h, float *out2);
+int pic_adjoint_free(pic_handle *h);
+
 /* Field energies without any allocation.  No counterpart in the reference.
  * For callers that cannot let the library call cudaMalloc (their framework
  * owns all device memory, or a timed loop cannot take cudaMalloc's implicit

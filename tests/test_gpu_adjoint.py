@@ -1,0 +1,123 @@
+"""Differentiable run (pic_forward / pic_backward) through the C ABI.
+
+1. pic_forward is the same time step as pic_step: fields within 1e-12
+   relative L2 and identical per-cell counts after the run (only the order of
+   the FP64 current sums differs).
+2. The adjoint gradient of L = sum over the last `window` steps of
+   h^3 sum E_x^2 matches FP64 central finite differences along seeded random
+   directions of the beam's initial momenta, and along the beam drift and
+   thermal spread: relative error below 1e-3 (see the FD test for the choice
+   of eps).
+3. The gradient does not depend on the checkpoint interval (segments
+   recomputed from different checkpoints give the same adjoint).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+H, TAU = 0.1, 0.02
+KEYS = ("x", "y", "z", "px", "py", "pz")
+
+
+def make(pkg, cells=(16, 8, 8), ppc=4, precision="fp64", seed=11):
+    sim = pkg.PicSimulation(cells, tuple(c * H for c in cells), TAU, pkg.configs.species_table(ppc),
+                            precision=precision)
+    for s, sp in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
+        sim.init_species(s, ppc, drift=sp["drift"], vth=sp["vth"], seed=seed + s)
+    return sim
+
+
+def rel_l2(a, b):
+    d = np.linalg.norm(a - b)
+    return 0.0 if d == 0.0 else d / max(np.linalg.norm(b), 1e-300)
+
+
+BEAM = 2
+STEPS, WINDOW = 30, 10
+LOSS = dict(field="Ex", window=WINDOW, species=BEAM, drift=(0.2, 0.0, 0.0), vth=0.002)
+
+
+def loss_with_beam(pkg, beam, precision="fp64"):
+    with make(pkg, precision=precision) as sim:
+        assert sim.load_particles(BEAM, *[beam[k] for k in KEYS]) == beam["x"].size
+        sim.forward(STEPS, STEPS)
+        return sim.loss_value(field="Ex", window=WINDOW)
+
+
+def fd_along(pkg, base, dp, eps=1e-6, precision="fp64"):
+    """central difference of L along the momentum perturbation dp (n, 3)"""
+    vals = []
+    for sgn in (1.0, -1.0):
+        b = {k: base[k].copy() for k in KEYS}
+        b["px"] = base["px"] + sgn * eps * dp[:, 0]
+        b["py"] = base["py"] + sgn * eps * dp[:, 1]
+        b["pz"] = base["pz"] + sgn * eps * dp[:, 2]
+        vals.append(loss_with_beam(pkg, b, precision))
+    return (vals[0] - vals[1]) / (2 * eps)
+
+
+def test_forward_is_the_step(pkg):
+    with make(pkg) as a, make(pkg) as b:
+        a.forward(12, 5)
+        b.run(12)
+        for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz"):
+            assert rel_l2(a.get_field(f), b.get_field(f)) < 1e-12, f
+        assert np.array_equal(a.cell_counts(), b.cell_counts())
+        hist = a.history()
+        assert hist.shape == (12, 3) and np.all(hist[-1] > 0)
+        ex = b.get_field("Ex").reshape(b.shape)[1:-1, 1:-1, 1:-1]
+        np.testing.assert_allclose(hist[-1, 0], H ** 3 * np.sum(ex * ex), rtol=1e-12)
+        # the state after pic_forward continues with pic_step
+        a.run(3)
+        b.run(3)
+        assert rel_l2(a.get_field("Ex"), b.get_field("Ex")) < 1e-12
+
+
+def test_gradient_matches_finite_differences(pkg):
+    """The reference's zigzag relay point (CurrentToMesh, cell.h:1306-1422) jumps
+    where a step switches between crossing one cell-centre plane (relay on the
+    trajectory) and two (relay pinned to both planes), so L is piecewise
+    smooth with small jumps.  A central difference whose +-eps interval holds
+    a jump is off by jump / (2 eps), whatever eps; the chance of one grows
+    with eps times the number of perturbed particles.  So: sparse random
+    directions (64 beam particles each) at eps = 1e-6, and dense directions
+    (every beam particle) at eps = 1e-8."""
+    with make(pkg) as sim:
+        base = sim.particles(BEAM)
+        sim.forward(STEPS, 7)
+        g = sim.backward(**LOSS)
+        L0 = sim.loss_value(field="Ex", window=WINDOW)
+    assert g["loss"] == L0
+    n = base["x"].size
+    assert g["d_p0"].shape == (n, 3)
+    rng = np.random.default_rng(2024)
+    errs = {}
+    for q in range(4):
+        v = np.zeros((n, 3))
+        idx = rng.choice(n, 64, replace=False)
+        v[idx] = rng.standard_normal((64, 3))
+        ad = float(np.sum(g["d_p0"] * v))
+        errs[f"sparse{q}"] = abs(fd_along(pkg, base, v, eps=1e-6) - ad) / abs(ad)
+    for q in range(2):
+        v = rng.standard_normal((n, 3))
+        ad = float(np.sum(g["d_p0"] * v))
+        errs[f"dense{q}"] = abs(fd_along(pkg, base, v, eps=1e-8) - ad) / abs(ad)
+    # drift (x) and thermal spread: p0 = drift + vth xi
+    e_x = np.zeros((n, 3))
+    e_x[:, 0] = 1.0
+    errs["drift"] = abs(fd_along(pkg, base, e_x, eps=1e-8) - g["d_drift"][0]) / abs(g["d_drift"][0])
+    xi = np.stack([base["px"] - 0.2, base["py"], base["pz"]], axis=1) / 0.002
+    errs["vth"] = abs(fd_along(pkg, base, xi, eps=1e-8) - g["d_vth"]) / abs(g["d_vth"])
+    assert max(errs.values()) < 1e-3, errs
+
+
+def test_gradient_independent_of_checkpoints(pkg):
+    grads = []
+    for K in (1, 7, STEPS):
+        with make(pkg) as sim:
+            sim.forward(STEPS, K)
+            grads.append(sim.backward(**LOSS))
+    for g in grads[1:]:
+        assert rel_l2(g["d_p0"], grads[0]["d_p0"]) < 1e-9
+        np.testing.assert_allclose(g["d_drift"], grads[0]["d_drift"], rtol=1e-9)
