@@ -755,11 +755,12 @@ __global__ void k_adj_ghosts(Grid g, GPasses P) {
 }
 
 // loss injection: lambda_E_c += 2 w E_c on nodes 1..N; history sums
-__global__ void k_inject(Grid g, const double *__restrict__ E, double *LE, double w2) {
+template <typename T>
+__global__ void k_inject(Grid g, const T *__restrict__ E, double *LE, double w2) {
     int k = blockIdx.x * blockDim.x + threadIdx.x, l = blockIdx.y, i = blockIdx.z;
     if (k < 1 || k > g.nz || l < 1 || l > g.ny || i < 1 || i > g.nx) return;
     size_t n = g.node(i, l, k);
-    LE[n] += w2 * E[n];
+    LE[n] += w2 * (double)E[n];
 }
 
 template <typename T>
@@ -1003,10 +1004,77 @@ void adj_free(pic_handle *h) {
 // ====================================================== host: forward ==
 namespace {
 
-int forward_plain(pic_handle *h, AdjState &A) {
+// field arrays of one state in the form's type: E, H (6 arrays)
+inline size_t field_bytes(const pic_handle *h) {
+    return h->g.nodes_pitched() * (h->mixed ? sizeof(float) : sizeof(double));
+}
+// recompute field set: E, H in the form's type, then J (and Q) in FP64
+void rf_view(pic_handle *h, AdjState &A, void *RF[PIC_FIELD_COUNT]) {
+    const size_t fb = field_bytes(h), db = h->g.nodes_pitched() * sizeof(double);
+    for (int a = 0; a < PIC_FIELD_COUNT; a++)
+        RF[a] = a < 6 ? A.rf + a * fb : A.rf + 6 * fb + (a - 6) * db;
+    if (h->mixed) RF[PIC_QX] = RF[PIC_QY] = RF[PIC_QZ] = nullptr;
+}
+
+MixParams mix_params(pic_handle *h, AdjState &A, char *state, void *const F[PIC_FIELD_COUNT], char *out) {
+    MixParams P;
+    memset(&P, 0, sizeof(P));
+    P.g = h->g;
+    P.nsp = A.nsp;
+    int *cell[kMaxSpecies];
+    void *v[kMaxSpecies][6];
+    adj_state_view(A, state, cell, v);
+    P.off[0] = 0;
+    for (int s = 0; s < A.nsp; s++) {
+        P.sp[s].n = A.n[s];
+        P.sp[s].q_m = h->sp[s].v.q_m;
+        P.sp[s].m = h->sp[s].v.m;
+        P.sp[s].cell = cell[s];
+        for (int a = 0; a < 6; a++) P.sp[s].v[a] = (float *)v[s][a];
+        P.off[s + 1] = P.off[s] + A.n[s];
+    }
+    adj_state_view(A, out ? out : state, cell, v);
+    for (int s = 0; s < A.nsp; s++) {
+        P.out[s].cell = cell[s];
+        for (int a = 0; a < 6; a++) P.out[s].v[a] = (float *)v[s][a];
+    }
+    for (int c = 0; c < 3; c++) {
+        P.E[c] = (const float *)F[PIC_EX + c];
+        P.H[c] = (const float *)F[PIC_HX + c];
+        P.J[c] = (double *)F[PIC_JX + c];
+    }
+    P.st = A.st;
+    return P;
+}
+
+// one forward step of the fixed-order state on the field set F: particles
+// read from `state`, written to `out` (same buffer when null); Fout, when
+// given, receives the interpolated fields of every particle
+int flat_step(pic_handle *h, AdjState &A, char *state, void *const F[PIC_FIELD_COUNT], char *out, void *Fout) {
+    if (!h->mixed) return flat_step_plain(h, A, state, F, out, (double *)Fout);
+    const Grid &g = h->g;
+    cudaStream_t s = h->stream;
+    float *const *E = (float *const *)&F[PIC_EX];
+    float *const *H = (float *const *)&F[PIC_HX];
+    yee_b_half_mixed(g, E, H, s);
+    const size_t nodes = g.nodes_pitched();
+    for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(F[PIC_JX + c], 0, nodes * sizeof(double), s), "zero J");
+    MixParams P = mix_params(h, A, state, F, out);
+    const int64_t n = total_particles(A);
+    for (int c = 0; c < 6; c++) P.Fout[c] = Fout ? (float *)Fout + (size_t)c * n : nullptr;
+    CK(launch_flat_push_mixed(P, s), "flat push");
+    j_fold(g, (double *)F[PIC_JX], (double *)F[PIC_JY], (double *)F[PIC_JZ], s);
+    yee_b_half_mixed(g, E, H, s);  // completion: the same Q again
+    yee_e_update_mixed(g, E, H, (double *const *)&F[PIC_JX], s);
+    e_ghosts_mixed(g, E[0], E[1], E[2], h->cfg.ghosts == PIC_GHOSTS_PERIODIC, s);
+    CK(cudaGetLastError(), "flat step fields");
+    return PIC_OK;
+}
+
+int forward_run(pic_handle *h, AdjState &A) {
     const Grid &g = h->g;
     cudaStream_t st = h->stream;
-    const size_t fbytes = g.nodes_pitched() * sizeof(double);
+    const size_t fbytes = field_bytes(h);
     CK(cudaEventRecord(A.e0, st), "event");
     for (int n = 0; n < A.steps; n++) {
         if (n % A.K == 0) {
@@ -1016,21 +1084,29 @@ int forward_plain(pic_handle *h, AdjState &A) {
                 CK(cudaMemcpyAsync(A.ckf + ((size_t)c * 6 + a) * fbytes, h->f[PIC_EX + a], fbytes,
                                    cudaMemcpyDeviceToDevice, st), "ckpt fields");
         }
-        int rc = flat_step_plain(h, A, A.cur, h->f);
+        int rc = flat_step(h, A, A.cur, h->f, nullptr, nullptr);
         if (rc) return rc;
-        k_history<double><<<node_grid(g), 32, 0, st>>>(g, (const double *)h->f[PIC_EX], (const double *)h->f[PIC_EY],
-                                                       (const double *)h->f[PIC_EZ], A.hist + 3 * n);
+        if (h->mixed)
+            k_history<float><<<node_grid(g), 32, 0, st>>>(g, (const float *)h->f[PIC_EX], (const float *)h->f[PIC_EY],
+                                                          (const float *)h->f[PIC_EZ], A.hist + 3 * n);
+        else
+            k_history<double><<<node_grid(g), 32, 0, st>>>(g, (const double *)h->f[PIC_EX],
+                                                           (const double *)h->f[PIC_EY],
+                                                           (const double *)h->f[PIC_EZ], A.hist + 3 * n);
         CK(cudaGetLastError(), "history");
     }
     CK(cudaEventRecord(A.e1, st), "event");
     return PIC_OK;
 }
 
-int reverse_step_plain(pic_handle *h, AdjState &A, const pic_loss &L, int n, char *state, double *const EHn,
-                       const double *Enext, const double *Fin) {
+// reverse of step n: EHn = E_n, H_n of the step (form's type, 6 arrays),
+// Enext = E after the step, Fin = the push's interpolated fields (or null)
+int reverse_step(pic_handle *h, AdjState &A, const pic_loss &L, int n, char *state, const char *EHn,
+                 const char *Enext, const void *Fin) {
     const Grid &g = h->g;
     cudaStream_t st = h->stream;
     const size_t N = g.nodes_pitched();
+    const size_t fb = field_bytes(h);
     double *LE[3], *LH[3], *LJ[3], *LQ[3];
     for (int c = 0; c < 3; c++) {
         LE[c] = A.lamf + (0 + c) * N;
@@ -1040,8 +1116,10 @@ int reverse_step_plain(pic_handle *h, AdjState &A, const pic_loss &L, int n, cha
     }
     // loss injection at E_{n+1}
     if (n >= A.steps - L.window) {
-        double w = g.hx * g.hy * g.hz;
-        k_inject<<<node_grid(g), 32, 0, st>>>(g, Enext + (size_t)L.field * N, LE[L.field], 2.0 * w);
+        double w2 = 2.0 * g.hx * g.hy * g.hz;
+        const char *Ec = Enext + (size_t)L.field * fb;
+        if (h->mixed) k_inject<float><<<node_grid(g), 32, 0, st>>>(g, (const float *)Ec, LE[L.field], w2);
+        else k_inject<double><<<node_grid(g), 32, 0, st>>>(g, (const double *)Ec, LE[L.field], w2);
     }
     // ghost copies (second launch first)
     GPasses GA, GB;
@@ -1062,50 +1140,74 @@ int reverse_step_plain(pic_handle *h, AdjState &A, const pic_loss &L, int n, cha
         int a = dir == 0 ? g.NY : g.NX, b = dir == 2 ? g.NY : g.NZ;
         k_adj_j_fold<<<(a * b + 127) / 128, 128, 0, st>>>(g, LJ[0], LJ[1], LJ[2], dir);
     }
-    // H_a of step n
-    const double *En = EHn, *Hn = EHn + 3 * N;
-    double *Ha = (double *)A.ha;
-    k_h_half<<<node_grid(g), 32, 0, st>>>(g, En, En + N, En + 2 * N, Hn, Hn + N, Hn + 2 * N, Ha, Ha + N, Ha + 2 * N,
-                                          FA.cx, FA.cy, FA.cz);
-    // particles
-    void *F[PIC_FIELD_COUNT] = {};
-    for (int c = 0; c < 3; c++) {
-        F[PIC_EX + c] = (void *)(En + c * N);
-        F[PIC_HX + c] = (void *)(Ha + c * N);
-    }
-    AdjParams P;
-    memset(&P, 0, sizeof(P));
-    P.f = flat_params(h, A, state, F);
-    size_t o = 0;
-    for (int s = 0; s < A.nsp; s++) {
-        for (int a = 0; a < 6; a++) P.lam[s].v[a] = (double *)A.lamp + o + (size_t)a * A.n[s];
-        o += 6 * (size_t)A.n[s];
-    }
-    for (int c = 0; c < 3; c++) { P.LJ[c] = LJ[c]; P.LE[c] = LE[c]; P.LH[c] = LH[c]; }
-    int64_t np = total_particles(A);
-    for (int c = 0; c < 6; c++) {
-        P.LF[c] = (double *)A.lamF + (size_t)c * np;
-        P.Fin[c] = Fin ? Fin + (size_t)c * np : nullptr;
-    }
-    if (np > 0) {
-        if (Fin) k_adj_push_plain<true><<<blocks_of(np), kT, 0, st>>>(P);
-        else k_adj_push_plain<false><<<blocks_of(np), kT, 0, st>>>(P);
-        k_adj_interp_plain<<<blocks_of(np), kT, 0, st>>>(P);
+    const int64_t np = total_particles(A);
+    if (!h->mixed) {
+        // H_a of step n
+        const double *En = (const double *)EHn, *Hn = (const double *)EHn + 3 * N;
+        double *Ha = (double *)A.ha;
+        k_h_half<<<node_grid(g), 32, 0, st>>>(g, En, En + N, En + 2 * N, Hn, Hn + N, Hn + 2 * N, Ha, Ha + N,
+                                              Ha + 2 * N, FA.cx, FA.cy, FA.cz);
+        void *F[PIC_FIELD_COUNT] = {};
+        for (int c = 0; c < 3; c++) {
+            F[PIC_EX + c] = (void *)(En + c * N);
+            F[PIC_HX + c] = (void *)(Ha + c * N);
+        }
+        AdjParams P;
+        memset(&P, 0, sizeof(P));
+        P.f = flat_params(h, A, state, F);
+        size_t o = 0;
+        for (int s = 0; s < A.nsp; s++) {
+            for (int a = 0; a < 6; a++) P.lam[s].v[a] = (double *)A.lamp + o + (size_t)a * A.n[s];
+            o += 6 * (size_t)A.n[s];
+        }
+        for (int c = 0; c < 3; c++) { P.LJ[c] = LJ[c]; P.LE[c] = LE[c]; P.LH[c] = LH[c]; }
+        for (int c = 0; c < 6; c++) {
+            P.LF[c] = (double *)A.lamF + (size_t)c * np;
+            P.Fin[c] = Fin ? (const double *)Fin + (size_t)c * np : nullptr;
+        }
+        if (np > 0) {
+            if (Fin) k_adj_push_plain<true><<<blocks_of(np), kT, 0, st>>>(P);
+            else k_adj_push_plain<false><<<blocks_of(np), kT, 0, st>>>(P);
+            k_adj_interp_plain<<<blocks_of(np), kT, 0, st>>>(P);
+        }
+    } else {
+        const float *En = (const float *)EHn, *Hn = (const float *)EHn + 3 * N;
+        float *Ha = (float *)A.ha;
+        CK(launch_h_half_mixed(g, En, Hn, Ha, N, st), "half step");
+        void *F[PIC_FIELD_COUNT] = {};
+        for (int c = 0; c < 3; c++) {
+            F[PIC_EX + c] = (void *)(En + c * N);
+            F[PIC_HX + c] = (void *)(Ha + c * N);
+        }
+        MixParams P = mix_params(h, A, state, F, nullptr);
+        size_t o = 0;
+        for (int s = 0; s < A.nsp; s++) {
+            for (int a = 0; a < 6; a++) P.lam[s][a] = (float *)A.lamp + o + (size_t)a * A.n[s];
+            o += 6 * (size_t)A.n[s];
+        }
+        for (int c = 0; c < 3; c++) { P.LJ[c] = LJ[c]; P.LE[c] = LE[c]; P.LH[c] = LH[c]; }
+        for (int c = 0; c < 6; c++) {
+            P.LF[c] = (float *)A.lamF + (size_t)c * np;
+            P.Fin[c] = Fin ? (const float *)Fin + (size_t)c * np : nullptr;
+        }
+        CK(launch_adj_particles_mixed(P, st), "adjoint particles");
     }
     k_adj_b_half<<<node_grid(g), 32, 0, st>>>(FA);
     CK(cudaGetLastError(), "reverse step");
     return PIC_OK;
 }
 
-int backward_plain(pic_handle *h, AdjState &A, const pic_loss &L) {
+int backward_run(pic_handle *h, AdjState &A, const pic_loss &L) {
     const Grid &g = h->g;
     cudaStream_t st = h->stream;
     const size_t N = g.nodes_pitched();
-    const size_t fbytes = N * sizeof(double);
+    const size_t fbytes = field_bytes(h);
+    const int64_t np = total_particles(A);
+    const size_t Fstep = (size_t)6 * np * A.elem;  // interpolated fields of one step
     CK(cudaMemsetAsync(A.lamp, 0, A.lamp_bytes, st), "zero lambda");
-    CK(cudaMemsetAsync(A.lamf, 0, 12 * fbytes, st), "zero lambda fields");
+    CK(cudaMemsetAsync(A.lamf, 0, 12 * N * sizeof(double), st), "zero lambda fields");
     void *RF[PIC_FIELD_COUNT];
-    for (int a = 0; a < PIC_FIELD_COUNT; a++) RF[a] = A.rf + a * fbytes;
+    rf_view(h, A, RF);
     CK(cudaEventRecord(A.e0, st), "event");
     for (int seg = A.nseg - 1; seg >= 0; seg--) {
         int start = seg * A.K, end = std::min(start + A.K, A.steps), len = end - start;
@@ -1115,17 +1217,16 @@ int backward_plain(pic_handle *h, AdjState &A, const pic_loss &L) {
         for (int j = 0; j < len; j++) {
             CK(cudaMemcpyAsync(A.segf + (size_t)j * 6 * fbytes, A.rf, 6 * fbytes, cudaMemcpyDeviceToDevice, st),
                "keep fields");
-            double *Fj = A.segF ? (double *)A.segF + (size_t)j * 6 * total_particles(A) : nullptr;
-            int rc = flat_step_plain(h, A, A.segp + (size_t)j * A.pbytes, RF, A.segp + (size_t)(j + 1) * A.pbytes, Fj);
+            void *Fj = A.segF ? (char *)A.segF + (size_t)j * Fstep : nullptr;
+            int rc = flat_step(h, A, A.segp + (size_t)j * A.pbytes, RF, A.segp + (size_t)(j + 1) * A.pbytes, Fj);
             if (rc) return rc;
         }
         CK(cudaMemcpyAsync(A.segf + (size_t)len * 6 * fbytes, A.rf, 6 * fbytes, cudaMemcpyDeviceToDevice, st),
            "keep fields");
         for (int j = len - 1; j >= 0; j--) {
-            int rc = reverse_step_plain(h, A, L, start + j, A.segp + (size_t)j * A.pbytes,
-                                        (double *)(A.segf + (size_t)j * 6 * fbytes),
-                                        (const double *)(A.segf + (size_t)(j + 1) * 6 * fbytes),
-                                        A.segF ? (const double *)A.segF + (size_t)j * 6 * total_particles(A) : nullptr);
+            int rc = reverse_step(h, A, L, start + j, A.segp + (size_t)j * A.pbytes, A.segf + (size_t)j * 6 * fbytes,
+                                  A.segf + (size_t)(j + 1) * 6 * fbytes,
+                                  A.segF ? (const char *)A.segF + (size_t)j * Fstep : nullptr);
             if (rc) return rc;
         }
     }
@@ -1198,7 +1299,7 @@ int pic_forward(pic_handle *h, int steps, int ckpt_every) {
         CK(cudaStreamSynchronize(h->stream), "sync");
     }
     cudaFree(d0);
-    rc = h->mixed ? adj_forward_mixed(h, A) : forward_plain(h, A);
+    rc = forward_run(h, A);
     if (rc) return rc;
     if ((rc = check_adj_status(h, A, "pic_forward"))) return rc;
     CK(cudaEventElapsedTime(&A.t_fwd, A.e0, A.e1), "timing");
@@ -1275,7 +1376,7 @@ int pic_backward(pic_handle *h, const pic_loss *loss, pic_grads *grads) {
         }
     }
     CK(cudaMemsetAsync(A.st, 0, sizeof(AdjStatus), h->stream), "zero status");
-    rc = h->mixed ? adj_backward_mixed(h, A, *loss) : backward_plain(h, A, *loss);
+    rc = backward_run(h, A, *loss);
     if (rc) return rc;
     if ((rc = check_adj_status(h, A, "pic_backward"))) return rc;
     CK(cudaEventElapsedTime(&A.t_bwd, A.e0, A.e1), "timing");

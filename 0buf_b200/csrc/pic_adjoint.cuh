@@ -55,11 +55,41 @@ inline size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 size_t adj_state_bytes(const AdjState &A);
 void adj_state_view(const AdjState &A, char *base, int *cell[kMaxSpecies], void *v[kMaxSpecies][6]);
 
-// FP32 form (pic_adjoint_mixed.cu)
+// ---- FP32 form (pic_adjoint_mixed.cu): particle kernels of the fixed-order pass
+struct MixSp {
+    int64_t n;
+    double q_m, m;
+    int *cell;     // packed cell
+    float *v[6];   // in-cell offsets (cell units) and momenta
+};
+struct MixOut {
+    int *cell;
+    float *v[6];
+};
+struct MixParams {
+    Grid g;
+    int nsp;
+    int64_t off[kMaxSpecies + 1];
+    MixSp sp[kMaxSpecies];      // state at the start of the step
+    MixOut out[kMaxSpecies];    // push: state after the step (may alias sp)
+    const float *E[3];
+    const float *H[3];          // push: H after the half step
+    double *J[3];
+    float *Fout[6];             // push, optional: interpolated fields per particle
+    AdjStatus *st;
+    // adjoint
+    float *lam[kMaxSpecies][6]; // lambda_x (cell units), lambda_p
+    const double *LJ[3];
+    double *LE[3], *LH[3];
+    float *LF[6];
+    const float *Fin[6];        // the push's interpolated fields of this step, or null
+};
+cudaError_t launch_flat_push_mixed(const MixParams &P, cudaStream_t s);
+cudaError_t launch_adj_particles_mixed(const MixParams &P, cudaStream_t s);
+// Ha = H + Q(E) in FP32 (the forward's half step, out of place); E, H, Ha: 3 arrays of N each
+cudaError_t launch_h_half_mixed(const Grid &g, const float *E, const float *H, float *Ha, size_t N, cudaStream_t s);
 void adj_gather_mixed(const Grid &g, const SpeciesView &S, const int64_t *d0, int *cell, void *const v[6],
                       cudaStream_t s);
-int adj_forward_mixed(pic_handle *h, AdjState &A);
-int adj_backward_mixed(pic_handle *h, AdjState &A, const pic_loss &L);
 // lambda_p (3 FP32 arrays of n) and p0 (3 FP32 arrays) -> 6 FP64 arrays of n
 void adj_widen_mixed(const float *lp, const float *const p0[3], int64_t n, double *out6, cudaStream_t s);
 

@@ -121,3 +121,37 @@ def test_gradient_independent_of_checkpoints(pkg):
     for g in grads[1:]:
         assert rel_l2(g["d_p0"], grads[0]["d_p0"]) < 1e-9
         np.testing.assert_allclose(g["d_drift"], grads[0]["d_drift"], rtol=1e-9)
+
+
+def test_mixed_forward_is_the_step(pkg):
+    """FP32 form: the fixed-order pass adds the current in FP64 without the
+    product push's 2^-22 warp quantum, so fields agree to FP32 level."""
+    with make(pkg, precision="fp32") as a, make(pkg, precision="fp32") as b:
+        a.forward(12, 5)
+        b.run(12)
+        for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz"):
+            assert rel_l2(a.get_field(f), b.get_field(f)) < 1e-4, f
+        assert np.abs(a.cell_counts() - b.cell_counts()).sum() <= 4
+        a.run(2)  # continues with the product step
+
+
+def test_mixed_gradient_matches_fp64(pkg):
+    """The FP32 adjoint (FP32 per particle, FP64 field adjoints) against the
+    FP64 adjoint and FP64 central differences of the same loss."""
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        with make(pkg, precision=prec) as sim:
+            if prec == "fp64":
+                base = sim.particles(BEAM)
+            sim.forward(STEPS, 7)
+            grads[prec] = sim.backward(**LOSS)
+    g64, g32 = grads["fp64"], grads["fp32"]
+    assert abs(g32["loss"] - g64["loss"]) / g64["loss"] < 1e-4
+    assert abs(g32["d_drift"][0] - g64["d_drift"][0]) / abs(g64["d_drift"][0]) < 1e-3
+    assert abs(g32["d_vth"] - g64["d_vth"]) / abs(g64["d_vth"]) < 1e-3
+    assert rel_l2(g32["d_p0"], g64["d_p0"]) < 1e-2
+    n = base["x"].size
+    e_x = np.zeros((n, 3))
+    e_x[:, 0] = 1.0
+    fd = fd_along(pkg, base, e_x, eps=1e-8)
+    assert abs(g32["d_drift"][0] - fd) / abs(fd) < 1e-3
