@@ -560,51 +560,93 @@ __global__ void __launch_bounds__(kT, 2) k_adj_push_plain(AdjParams A) {
 // ---- adjoint of the interpolation (second pass, few registers): scatter
 // lambda_F into lambda_E / lambda_H and add F's position gradient to lambda_x
 __global__ void __launch_bounds__(kT) k_adj_interp_plain(AdjParams A) {
+    __shared__ int sHi[6 * kBoxNodes], sLo[6 * kBoxNodes];
+    __shared__ int sRed[6 * (kT / 32)];
+    __shared__ unsigned sMax[kT / 32], sMaxOut;
+    __shared__ NodeBox sBox;
     const FlatParams &P = A.f;
-    int64_t idx = spread_index(threadIdx.x);
-    if (idx >= P.off[P.nsp]) return;
     const Grid &g = P.g;
-    int s = species_of(P.off, P.nsp, idx);
-    const FlatSp &S = P.sp[s];
-    int64_t j = idx - P.off[s];
-    double x[3] = {S.v[0][j], S.v[1][j], S.v[2][j]};
-    if (x[0] < 0 || x[1] < 0 || x[2] < 0) return;  // the push saw zero fields
-    int i, l, k;
-    g.cell_ijk(S.cell[j], i, l, k);
-    Taps T;
-    taps_plain(g, i, l, k, x, T);
-    const size_t dX = (size_t)g.NY * g.pz, dY = g.pz, dZ = 1;
-    double gx[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int c = 0; c < 6; c++) {
-        int t[3];
-        double w[3];
-        const double lam = A.LF[c][idx];
-        if (!comp_taps(T, c, t, w) || lam == 0.0) continue;
-        size_t n = tap_node(g, i, l, k, t);
-        const double *Arr = c < 3 ? P.E[c] : P.H[c - 3];
-        double *LA = c < 3 ? A.LE[c] : A.LH[c - 3];
-        const double W0[2] = {w[0], 1. - w[0]}, W1[2] = {w[1], 1. - w[1]}, W2[2] = {w[2], 1. - w[2]};
-        double gr[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int a = 0; a < 2; a++)
-#pragma unroll
-            for (int bb = 0; bb < 2; bb++)
-#pragma unroll
-                for (int cc = 0; cc < 2; cc++) {
-                    size_t m = n + a * dX + bb * dY + cc * dZ;
-                    double v = Arr[m];
-                    atomicAdd(&LA[m], lam * (W0[a] * W1[bb] * W2[cc]));
-                    gr[0] += (a ? 1.0 : -1.0) * W1[bb] * W2[cc] * v;
-                    gr[1] += (bb ? 1.0 : -1.0) * W0[a] * W2[cc] * v;
-                    gr[2] += (cc ? 1.0 : -1.0) * W0[a] * W1[bb] * v;
-                }
-        gx[0] += lam * gr[0] / g.hx;
-        gx[1] += lam * gr[1] / g.hy;
-        gx[2] += lam * gr[2] / g.hz;
+    int64_t idx = spread_index(threadIdx.x);
+    bool valid = idx < P.off[P.nsp];
+    int s = 0, i = 0, l = 0, k = 0;
+    int64_t j = 0;
+    double x[3] = {0.0, 0.0, 0.0};
+    if (valid) {
+        s = species_of(P.off, P.nsp, idx);
+        const FlatSp &S = P.sp[s];
+        j = idx - P.off[s];
+        x[0] = S.v[0][j]; x[1] = S.v[1][j]; x[2] = S.v[2][j];
+        g.cell_ijk(S.cell[j], i, l, k);
+        valid = !(x[0] < 0 || x[1] < 0 || x[2] < 0);  // else the push saw zero fields
     }
-    const LamSp &Lm = A.lam[s];
-    for (int d = 0; d < 3; d++) Lm.v[d][j] += gx[d];
+    double lam6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    float amax = 0.f;
+    if (valid) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            lam6[c] = A.LF[c][idx];
+            amax = fmaxf(amax, (float)fabs(lam6[c]));
+        }
+    }
+    const NodeBox box = block_node_box(i, l, k, valid, sRed, &sBox);
+    const float bmax = block_max_abs(amax, sMax, &sMaxOut);
+    if (bmax == 0.f) return;  // no adjoint reaches the particles of this block
+    const int E = box_exponent(bmax);
+    const double inv_q = pow2_d(22 - E);
+    for (int e = threadIdx.x; e < 6 * box.nodes; e += blockDim.x) sHi[e] = sLo[e] = 0;
+    __syncthreads();
+    if (valid) {
+        Taps T;
+        taps_plain(g, i, l, k, x, T);
+        const size_t dX = (size_t)g.NY * g.pz, dY = g.pz, dZ = 1;
+        double gx[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            int t[3];
+            double w[3];
+            const double lam = lam6[c];
+            if (!comp_taps(T, c, t, w) || lam == 0.0) continue;
+            size_t n = tap_node(g, i, l, k, t);
+            const double *Arr = c < 3 ? P.E[c] : P.H[c - 3];
+            double *LA = c < 3 ? A.LE[c] : A.LH[c - 3];
+            const int b0 = box.nodes ? c * box.nodes + box_index(box, i + t[0] - 2, l + t[1] - 2, k + t[2] - 2) : 0;
+            const double W0[2] = {w[0], 1. - w[0]}, W1[2] = {w[1], 1. - w[1]}, W2[2] = {w[2], 1. - w[2]};
+            double gr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+                    for (int cc = 0; cc < 2; cc++) {
+                        size_t m = n + a * dX + bb * dY + cc * dZ;
+                        double v = Arr[m];
+                        double add = lam * (W0[a] * W1[bb] * W2[cc]);
+                        if (box.nodes) {
+                            const int e = b0 + (a * box.by + bb) * box.bz + cc;
+                            double vq = add * inv_q;
+                            int hi = __double2int_rn(vq);
+                            int lo = __double2int_rn((vq - (double)hi) * 0x1p22);
+                            if (hi) atomicAdd(&sHi[e], hi);
+                            if (lo) atomicAdd(&sLo[e], lo);
+                        } else {
+                            atomicAdd(&LA[m], add);
+                        }
+                        gr[0] += (a ? 1.0 : -1.0) * W1[bb] * W2[cc] * v;
+                        gr[1] += (bb ? 1.0 : -1.0) * W0[a] * W2[cc] * v;
+                        gr[2] += (cc ? 1.0 : -1.0) * W0[a] * W1[bb] * v;
+                    }
+            gx[0] += lam * gr[0] / g.hx;
+            gx[1] += lam * gr[1] / g.hy;
+            gx[2] += lam * gr[2] / g.hz;
+        }
+        const LamSp &Lm = A.lam[s];
+        for (int d = 0; d < 3; d++) Lm.v[d][j] += gx[d];
+    }
+    if (box.nodes) {
+        __syncthreads();
+        double *const dst[6] = {A.LE[0], A.LE[1], A.LE[2], A.LH[0], A.LH[1], A.LH[2]};
+        flush_node_box(box, sHi, sLo, pow2_d(E - 22), g, dst);
+    }
 }
 
 // ------------------------------------------------------------- fields --

@@ -407,51 +407,89 @@ __global__ void __launch_bounds__(kT, 2) k_adj_push_mixed(MixParams P) {
 
 // ---- adjoint, second pass: interpolation transpose
 __global__ void __launch_bounds__(kT) k_adj_interp_mixed(MixParams P) {
-    int64_t idx = spread_index(threadIdx.x);
-    if (idx >= P.off[P.nsp]) return;
+    __shared__ int sHi[6 * kBoxNodes];
+    __shared__ int sRed[6 * (kT / 32)];
+    __shared__ unsigned sMax[kT / 32], sMaxOut;
+    __shared__ NodeBox sBox;
     const Grid &g = P.g;
-    int s = species_of(P.off, P.nsp, idx);
-    const MixSp &S = P.sp[s];
-    int64_t j = idx - P.off[s];
-    float xs[3] = {S.v[0][j], S.v[1][j], S.v[2][j]};
-    int i, l, k;
-    g.cell_ijk(S.cell[j], i, l, k);
-    MTaps T;
-    taps_mixed(xs, T);
-    const size_t dX = (size_t)g.NY * g.pz, dY = g.pz, dZ = 1;
-    float gx[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int c = 0; c < 6; c++) {
-        int t[3];
-        float w[3];
-        const float lam = P.LF[c][idx];
-        if (lam == 0.f) continue;
-        comp_taps_m(T, c, t, w);
-        size_t n = tap_node(g, i, l, k, t);
-        const float *Arr = c < 3 ? P.E[c] : P.H[c - 3];
-        double *LA = c < 3 ? P.LE[c] : P.LH[c - 3];
-        const float W0[2] = {w[0], 1.f - w[0]}, W1[2] = {w[1], 1.f - w[1]}, W2[2] = {w[2], 1.f - w[2]};
-        float gr[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-        for (int a = 0; a < 2; a++)
-#pragma unroll
-            for (int bb = 0; bb < 2; bb++)
-#pragma unroll
-                for (int cc = 0; cc < 2; cc++) {
-                    size_t m = n + a * dX + bb * dY + cc * dZ;
-                    float v = Arr[m];
-                    atomicAdd(&LA[m], (double)(lam * (W0[a] * W1[bb] * W2[cc])));
-                    gr[0] += (a ? 1.f : -1.f) * W1[bb] * W2[cc] * v;
-                    gr[1] += (bb ? 1.f : -1.f) * W0[a] * W2[cc] * v;
-                    gr[2] += (cc ? 1.f : -1.f) * W0[a] * W1[bb] * v;
-                }
-        gx[0] += lam * gr[0];
-        gx[1] += lam * gr[1];
-        gx[2] += lam * gr[2];
+    int64_t idx = spread_index(threadIdx.x);
+    const bool valid = idx < P.off[P.nsp];
+    int s = 0, i = 0, l = 0, k = 0;
+    int64_t j = 0;
+    float xs[3] = {0.f, 0.f, 0.f};
+    if (valid) {
+        s = species_of(P.off, P.nsp, idx);
+        const MixSp &S = P.sp[s];
+        j = idx - P.off[s];
+        xs[0] = S.v[0][j]; xs[1] = S.v[1][j]; xs[2] = S.v[2][j];
+        g.cell_ijk(S.cell[j], i, l, k);
     }
-    float *const *Lm = P.lam[s];
+    float lam6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float amax = 0.f;
+    if (valid) {
 #pragma unroll
-    for (int d = 0; d < 3; d++) Lm[d][j] += gx[d];
+        for (int c = 0; c < 6; c++) {
+            lam6[c] = P.LF[c][idx];
+            amax = fmaxf(amax, fabsf(lam6[c]));
+        }
+    }
+    const NodeBox box = block_node_box(i, l, k, valid, sRed, &sBox);
+    const float bmax = block_max_abs(amax, sMax, &sMaxOut);
+    if (bmax == 0.f) return;  // no adjoint reaches the particles of this block
+    const int E = box_exponent(bmax);
+    const float inv_q = __uint_as_float((unsigned)(22 - E + 127) << 23);
+    for (int e = threadIdx.x; e < 6 * box.nodes; e += blockDim.x) sHi[e] = 0;
+    __syncthreads();
+    if (valid) {
+        MTaps T;
+        taps_mixed(xs, T);
+        const size_t dX = (size_t)g.NY * g.pz, dY = g.pz, dZ = 1;
+        float gx[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            int t[3];
+            float w[3];
+            const float lam = lam6[c];
+            if (lam == 0.f) continue;
+            comp_taps_m(T, c, t, w);
+            size_t n = tap_node(g, i, l, k, t);
+            const float *Arr = c < 3 ? P.E[c] : P.H[c - 3];
+            double *LA = c < 3 ? P.LE[c] : P.LH[c - 3];
+            const int b0 = box.nodes ? c * box.nodes + box_index(box, i + t[0] - 2, l + t[1] - 2, k + t[2] - 2) : 0;
+            const float W0[2] = {w[0], 1.f - w[0]}, W1[2] = {w[1], 1.f - w[1]}, W2[2] = {w[2], 1.f - w[2]};
+            float gr[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+                    for (int cc = 0; cc < 2; cc++) {
+                        size_t m = n + a * dX + bb * dY + cc * dZ;
+                        float v = Arr[m];
+                        float add = lam * (W0[a] * W1[bb] * W2[cc]);
+                        if (box.nodes) {
+                            int hi = __float2int_rn(add * inv_q);
+                            if (hi) atomicAdd(&sHi[b0 + (a * box.by + bb) * box.bz + cc], hi);
+                        } else {
+                            atomicAdd(&LA[m], (double)add);
+                        }
+                        gr[0] += (a ? 1.f : -1.f) * W1[bb] * W2[cc] * v;
+                        gr[1] += (bb ? 1.f : -1.f) * W0[a] * W2[cc] * v;
+                        gr[2] += (cc ? 1.f : -1.f) * W0[a] * W1[bb] * v;
+                    }
+            gx[0] += lam * gr[0];
+            gx[1] += lam * gr[1];
+            gx[2] += lam * gr[2];
+        }
+        float *const *Lm = P.lam[s];
+#pragma unroll
+        for (int d = 0; d < 3; d++) Lm[d][j] += gx[d];
+    }
+    if (box.nodes) {
+        __syncthreads();
+        double *const dst[6] = {P.LE[0], P.LE[1], P.LE[2], P.LH[0], P.LH[1], P.LH[2]};
+        flush_node_box(box, sHi, nullptr, pow2_d(E - 22), g, dst);
+    }
 }
 
 __global__ void k_h_half_m(Grid g, const float *__restrict__ Ex, const float *__restrict__ Ey,

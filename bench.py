@@ -290,9 +290,108 @@ def run_ours(args, dist):
 
     if not args.no_e2e:
         out["e2e"] = run_e2e(args, dist, pkg, cfg, form, torch, n_local)
+    if dist.world == 1 and not args.no_adjoint:
+        out["adjoint"] = run_adjoint(args, pkg, dev)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
+
+
+ADJ_LOSS = dict(field="Ex", window=50, species=2, drift=(0.2, 0.0, 0.0), vth=0.002)
+
+
+def run_adjoint(args, pkg, dev):
+    """The differentiable run at the adjoint configuration (128x32x32 cells,
+    32 particles/cell/species, 300 steps, checkpoints every 25): device time of
+    pic_forward and pic_backward in both forms, and the gradient of
+    L = sum over the last 50 steps of h^3 sum E_x^2 against FP64 central
+    differences of the FP64 forward -- along the beam drift and thermal spread
+    (every beam particle moves: small eps, see below) and along random single-particle
+    momentum directions (eps 1e-6).  Directions that move many particles at
+    eps 1e-6 are not used: the reference's zigzag relay point makes L jump
+    where a step changes from one to two crossed cell-centre planes, and such a
+    difference measures the jump, not the gradient; the thermal-spread direction
+    uses the median of three small eps for the same reason."""
+    import numpy as np
+    cfg = dict(pkg.configs.CONFIGS["c3"])
+    steps, K = cfg["steps"], 25
+    out = {"config": f"c3: {'x'.join(map(str, cfg['cells']))} cells, {cfg['ppc']} particles/cell/species x 3, "
+                     f"{steps} steps, checkpoints every {K}, loss = sum over the last 50 steps of h^3 sum E_x^2, "
+                     "gradient w.r.t. the beam's initial momenta, drift and thermal spread"}
+    grads = {}
+    base = None
+    for form in ("fp64", "fp32"):
+        sim = make_sim(pkg, cfg, form, dev, 0)
+        if form == "fp64":
+            base = sim.particles(ADJ_LOSS["species"])
+        sim.forward(steps, K)
+        g = sim.backward(**ADJ_LOSS)
+        t = sim.adjoint_timings()
+        sim.close()
+        grads[form] = g
+        out[form] = {"forward_ms": round(float(t[0]), 2), "backward_ms": round(float(t[1]), 2),
+                     "backward_over_forward": round(float(t[1] / t[0]), 3),
+                     "particle_steps_per_s_forward": round(sim_particles(cfg) * steps / (float(t[0]) / 1e3), 1),
+                     "loss": g["loss"], "d_drift_x": float(g["d_drift"][0]), "d_vth": float(g["d_vth"])}
+    keys = ("x", "y", "z", "px", "py", "pz")
+
+    def loss_of(dp, eps):
+        vals = []
+        for sg in (1.0, -1.0):
+            sim = make_sim(pkg, cfg, "fp64", dev, 0)
+            b = {k: base[k] for k in keys}
+            for a, k in enumerate(("px", "py", "pz")):
+                b[k] = base[k] + sg * eps * dp[:, a]
+            sim.load_particles(ADJ_LOSS["species"], *[b[k] for k in keys])
+            sim.forward(steps, steps)
+            vals.append(sim.loss_value(field="Ex", window=ADJ_LOSS["window"]))
+            sim.close()
+        return (vals[0] - vals[1]) / (2 * eps)
+
+    n = base["x"].size
+    # run-to-run spread of L (FP64 atomics add the current in no fixed order)
+    sim = make_sim(pkg, cfg, "fp64", dev, 0)
+    sim.forward(steps, steps)
+    out["loss_rerun_rel_diff"] = float(f"{abs(sim.loss_value(field='Ex', window=50) - grads['fp64']['loss']) / grads['fp64']['loss']:.3e}")
+    sim.close()
+    fd = {}
+    e_x = np.zeros((n, 3))
+    e_x[:, 0] = 1.0
+    xi = np.stack([base["px"] - 0.2, base["py"], base["pz"]], axis=1) / ADJ_LOSS["vth"]
+    d_drift = loss_of(e_x, 1e-8)
+    # the spread direction moves every beam particle with random signs: its
+    # signal is ~1000x below the drift's while it meets as many jumps, so take
+    # the median of three small eps (one jump spoils at most one of them)
+    vth_eps = (1e-9, 1e-10, 1e-11)
+    vth_fd = [loss_of(xi, e) for e in vth_eps]
+    d_vth = float(np.median(vth_fd))
+    out["fd_vth_by_eps"] = {f"{e:g}": v for e, v in zip(vth_eps, vth_fd)}
+    for form in ("fp64", "fp32"):
+        g = grads[form]
+        fd[form] = {"drift_rel_err": abs(g["d_drift"][0] - d_drift) / abs(d_drift),
+                    "vth_rel_err": abs(g["d_vth"] - d_vth) / abs(d_vth), "particle_dirs_rel_err": []}
+    rng = np.random.default_rng(16)
+    for _ in range(args.adjoint_dirs):
+        v = np.zeros((n, 3))
+        v[rng.integers(n)] = rng.standard_normal(3)
+        f = loss_of(v, 1e-6)
+        for form in ("fp64", "fp32"):
+            ad = float(np.sum(grads[form]["d_p0"] * v))
+            fd[form]["particle_dirs_rel_err"].append(abs(ad - f) / abs(f))
+    for form in fd:
+        errs = [fd[form]["drift_rel_err"], fd[form]["vth_rel_err"]] + fd[form]["particle_dirs_rel_err"]
+        fd[form]["max_rel_err"] = max(errs)
+        for k in list(fd[form]):
+            v = fd[form][k]
+            fd[form][k] = [float(f"{x:.3e}") for x in v] if isinstance(v, list) else float(f"{v:.3e}")
+    out["fd_check"] = {"reference": "FP64 central differences of the FP64 forward", "fd_drift": d_drift,
+                       "fd_vth": d_vth, **fd}
+    return out
+
+
+def sim_particles(cfg) -> int:
+    c = cfg["cells"]
+    return int(c[0] * c[1] * c[2] * cfg["ppc"] * 3)
 
 
 def run_e2e(args, dist, pkg, cfg, form, torch, n_local):
@@ -444,6 +543,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-run section")
+    ap.add_argument("--adjoint-dirs", type=int, default=4,
+                    help="random single-particle directions of the finite-difference check")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--reference-inner", type=int, default=20)
     args = ap.parse_args()
