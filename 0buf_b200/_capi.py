@@ -99,6 +99,7 @@ SIGNATURES = {
     "pic_error_string": (C.c_char_p, [C.c_int]),
     "pic_step_counters": (C.c_int, [H, I64]),
     "pic_step_timings": (C.c_int, [H, F]),
+    "pic_sort_stats": (C.c_int, [H, I64]),
     "pic_layout_info": (C.c_int, [H, I64]),
     "pic_stream": (C.c_void_p, [H]),
     "pic_forward": (C.c_int, [H, C.c_int, C.c_int]),

@@ -59,7 +59,18 @@ StepParams make_params(pic_handle *h) {
     return p;
 }
 
+void free_alt(pic_handle *h, int s) {
+    auto &S = h->sp[s];
+    if (S.alt_cell) cudaFree(S.alt_cell);
+    for (float *&a : S.alt) {
+        if (a) cudaFree(a);
+        a = nullptr;
+    }
+    S.alt_cell = nullptr;
+}
+
 void free_species(pic_handle *h, int s) {
+    free_alt(h, s);
     SpeciesView &v = h->sp[s].v;
     void *ptrs[] = {v.x, v.y, v.z, v.px, v.py, v.pz, v.ox, v.oy, v.oz, v.fx, v.fy, v.fz, v.cell, v.tile_start,
                     v.tile_count};
@@ -100,6 +111,10 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
     } else {
         float **arr[6] = {&v.ox, &v.oy, &v.oz, &v.fx, &v.fy, &v.fz};
         for (auto a : arr) CK(cudaMalloc(a, n * sizeof(float)), "alloc particles");
+        // second set for the per-tile cell sort (maybe_sort), allocated with the bins
+        auto &S = h->sp[s];
+        CK(cudaMalloc(&S.alt_cell, n * sizeof(int)), "alloc sort buffer");
+        for (float *&a : S.alt) CK(cudaMalloc(&a, n * sizeof(float)), "alloc sort buffer");
     }
     CK(cudaMalloc(&v.tile_start, (g.ntiles + 1) * sizeof(int)), "alloc tile_start");
     CK(cudaMalloc(&v.tile_count, g.ntiles * sizeof(int)), "alloc tile_count");
@@ -271,6 +286,33 @@ int check_status(pic_handle *h) {
     return PIC_OK;
 }
 
+// FP32 form: sort every species' tile bins by cell (into the alternate
+// arrays, then swap) when the last push found more than 2% of its particles
+// outside their warp's lead cell -- the deposit's fast path needs sorted bins
+int maybe_sort(pic_handle *h) {
+    h->sorts = 0;
+    if (!h->mixed) return PIC_OK;
+    int64_t total = 0;
+    for (int s = 0; s < h->cfg.nspecies; s++) total += h->sp[s].cap_total;
+    if ((double)h->st_host->unsorted <= 0.02 * (double)total) return PIC_OK;
+    for (int s = 0; s < h->cfg.nspecies; s++) {
+        auto &S = h->sp[s];
+        if (!S.loaded || S.cap_total == 0) continue;
+        if (!S.alt_cell) continue;
+        SpeciesView D = S.v;
+        D.cell = S.alt_cell;
+        float **dp[6] = {&D.ox, &D.oy, &D.oz, &D.fx, &D.fy, &D.fz};
+        for (int a = 0; a < 6; a++) *dp[a] = S.alt[a];
+        CK(sort_bins_f(h->g, S.v, D, h->stream), "sort bins");
+        std::swap(S.v.cell, S.alt_cell);
+        float **vp[6] = {&S.v.ox, &S.v.oy, &S.v.oz, &S.v.fx, &S.v.fy, &S.v.fz};
+        for (int a = 0; a < 6; a++) std::swap(*vp[a], S.alt[a]);
+        h->launches += 1;
+        h->sorts += 1;
+    }
+    return PIC_OK;
+}
+
 int need_particles(pic_handle *h) {
     for (int s = 0; s < h->cfg.nspecies; s++)
         if (!h->sp[s].loaded) {
@@ -427,12 +469,12 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
         h->sp[s].loaded = 0;
         h->sp[s].cap_total = 0;
     }
-    size_t smem = h->mixed ? push_smem_mixed(g) : push_smem_plain(g);
-    int optin = 0;
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-    if ((int)smem > optin) { delete h; return PIC_ERR_ARG; }
     int rc = set_device(h);
     if (rc) { delete h; return rc; }
+    size_t smem = h->mixed ? push_smem_total_mixed(g) : push_smem_plain(g);
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    if (smem > (size_t)optin) { delete h; return PIC_ERR_ARG; }
     auto fail = [&](cudaError_t e) { pic_destroy(h); return e == cudaErrorMemoryAllocation ? PIC_ERR_NOMEM : (int)e; };
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e) { delete h; return (int)e; }
@@ -694,6 +736,7 @@ int pic_step(pic_handle *h, int nt) {
     if ((rc = do_e_ghosts(h))) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     rc = check_status(h);
+    if (!rc) rc = maybe_sort(h);
     h->counters[3] = h->launches;
     if (!rc) {
         cudaEventElapsedTime(&h->timings[0], h->ev[0], h->ev[1]);
@@ -879,6 +922,13 @@ const char *pic_error_string(int status) {
 int pic_step_counters(pic_handle *h, int64_t *out4) {
     if (!h || !out4) return PIC_ERR_ARG;
     for (int i = 0; i < 4; i++) out4[i] = h->counters[i];
+    return PIC_OK;
+}
+
+int pic_sort_stats(pic_handle *h, int64_t *out2) {
+    if (!h || !out2) return PIC_ERR_ARG;
+    out2[0] = h->mixed && h->st_host ? (int64_t)h->st_host->unsorted : 0;
+    out2[1] = h->sorts;
     return PIC_OK;
 }
 

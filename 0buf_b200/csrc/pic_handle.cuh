@@ -26,7 +26,12 @@ struct pic_handle {
         int64_t cap_total;
         int loaded;
         std::vector<int> h_start;
+        // FP32 form: second set of particle arrays (same capacity) that the
+        // per-tile cell sort writes into before the two sets swap
+        int *alt_cell;
+        float *alt[6];
     } sp[pic::kMaxSpecies];
+    int64_t sorts;  // tile sorts run by the last step
     void *outbox;
     unsigned out_cap;
     size_t out_elem;

@@ -45,7 +45,8 @@ struct DevStatus {
     unsigned long long dropped;
     unsigned long long duplicated;
     double kinetic;            // sum (m/q_m)(gamma-1) accumulated by the push
-    double pad1[3];
+    unsigned long long unsorted;  // mixed push: particles outside their warp's lead cell (bins out of cell order)
+    double pad1[2];
 };
 
 struct Grid {

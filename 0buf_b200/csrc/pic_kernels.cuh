@@ -22,6 +22,8 @@ cudaError_t place_particles_plain(const Grid &g, int64_t n, const double *x, con
 void yee_b_half_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s);
 void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], double *const J[3], cudaStream_t s);
 size_t push_smem_mixed(const Grid &g);
+// dynamic + static shared memory of the mixed push kernel ((size_t)-1 if it cannot be queried)
+size_t push_smem_total_mixed(const Grid &g);
 cudaError_t launch_push_mixed(const StepParams &p, cudaStream_t s);
 
 // form-independent (pic_common.cu, FP64 parts with -fmad=false)
@@ -35,6 +37,8 @@ cudaError_t scatter_to_bins_f(const Grid &g, int mixed, int64_t n, const int *ce
                               int *fill, cudaStream_t s);
 cudaError_t gather_from_bins_f(const Grid &g, int mixed, SpeciesView sv, const int64_t *dense_start, int *cell,
                                float *ox, float *oy, float *oz, float *px, float *py, float *pz, cudaStream_t s);
+// FP32 form: sort each tile's bin by cell from src's arrays into dst's (same tile layout)
+cudaError_t sort_bins_f(const Grid &g, const SpeciesView &src, const SpeciesView &dst, cudaStream_t s);
 // flat device list -> per-tile counts of valid particles (cell >= 0)
 cudaError_t tile_histogram(const Grid &g, int64_t n, const int *cell, int *tile_counts, cudaStream_t s);
 // flat FP64 list -> bins of one species (plain or mixed), fill[] = running counts

@@ -53,14 +53,17 @@ __global__ void k_e_update_mixed(Grid g, float *Ex, float *Ey, float *Ez, const 
 }
 
 // ------------------------------------------------------- particle push --
-// Interpolate3D (cell.h:1054-1153) in cell units on the FP32 tile
-__device__ __forceinline__ float interp_mixed(const float *__restrict__ T, int SY, int SZ, int n0, int i, int l,
+// Interpolate3D (cell.h:1054-1153) in cell units on the FP32 tile, stored as
+// yz-quads: Q[n] = (T[n], T[n+dz], T[n+dy], T[n+dy+dz]), so the 8 taps are two
+// 128-bit shared loads (the same products and sums, in the same order, as
+// the 8 scalar taps)
+__device__ __forceinline__ float interp_mixed(const float4 *__restrict__ Q, int SY, int SZ, int n0, int i, int l,
                                               int k, float sx, float sy, float sz) {
-    int n = n0 + (i * SY + l) * SZ + k;
-    int dz = 1, dy = SZ, dx = SY * SZ;
-    float sx1 = 1.f - sx, sy1 = 1.f - sy, sz1 = 1.f - sz;
-    float t1 = sx * (sy * (sz * T[n] + sz1 * T[n + dz]) + sy1 * (sz * T[n + dy] + sz1 * T[n + dy + dz]));
-    float t2 = sx1 * (sy * (sz * T[n + dx] + sz1 * T[n + dx + dz]) + sy1 * (sz * T[n + dx + dy] + sz1 * T[n + dx + dy + dz]));
+    const int n = n0 + (i * SY + l) * SZ + k;
+    const float4 A = Q[n], B = Q[n + SY * SZ];
+    const float sx1 = 1.f - sx, sy1 = 1.f - sy, sz1 = 1.f - sz;
+    float t1 = sx * (sy * (sz * A.x + sz1 * A.y) + sy1 * (sz * A.z + sz1 * A.w));
+    float t2 = sx1 * (sy * (sz * B.x + sz1 * B.y) + sy1 * (sz * B.z + sz1 * B.w));
     return t1 + t2;
 }
 
@@ -130,10 +133,9 @@ __device__ __forceinline__ void split_point(const int i1[3], const int i2[3], co
     for (int d = 0; d < 3; d++) x2[d] = (i1[d] != i2[d]) ? 0.5f : xs[d] + (xe[d] - xs[d]) * sr;
 }
 
-// 2^e as float and double by exponent bits (no library call, no branch);
+// 2^e as float by exponent bits (no library call, no branch);
 // valid for -126 < e < 128
 __device__ __forceinline__ float pow2f(int e) { return __uint_as_float((unsigned)(e + 127) << 23); }
-__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 // e with 2^(e-1) <= x < 2^e for a positive normal float (0 for x = 0)
 __device__ __forceinline__ int exponent_above(float x) {
     return x > 0.f ? (int)((__float_as_uint(x) >> 23) & 0xff) - 126 : 0;
@@ -154,15 +156,30 @@ __device__ __forceinline__ PartM load_part(const SpeciesView &S, int slot) {
 }
 
 // Deposit of the warp's current, two levels:
-//  1. lanes whose particle sits in the warp's lead cell add their contributions
-//     into a per-warp int32 scratch indexed by (cell-centre class, contribution)
-//     -- native 32-bit shared atomics, 96 words.  The warp's quantum q_w is a
-//     power of two above 64 x the largest possible contribution of any of its
-//     lanes (1.0834 |current of the full step|, reduced with redux.sync), so the
-//     int32 sums cannot overflow; rounding is below FP32 precision of that bound;
-//  2. the <= 96 distinct per-warp sums go into the tile's exact 64-bit
-//     fixed-point J (fx_add) -- no conflicts between lanes.
-// Lanes in other cells (unsorted bins) add straight into the tile J.
+//  1. the depositing lanes form one group per distinct cell (match.any); for
+//     up to kGroups groups per warp, lanes add the first zigzag segment of
+//     their particle into a per-warp int32 scratch of 54 node slots per group
+//     -- the nodes that the segments of a particle in one cell can reach (Jx
+//     2x3x3, Jy 3x2x3, Jz 3x3x2 around the cell's stencil origin) -- with
+//     native 32-bit shared atomics.  The warp's quantum q_w is a power of two
+//     above 2^-22 x the largest possible contribution of any of its lanes
+//     (1.0834 |current of the full step|, reduced with redux.sync), so the
+//     int32 sums of <= 32 contributions cannot overflow.  The <= 54 sums per
+//     group then go into the tile's exact 64-bit fixed-point J (fx_add).
+//  2. segments that do not fit that pattern -- the second segment of a
+//     particle that crosses a cell-centre plane, and both segments of a lane
+//     beyond kGroups distinct cells (bins out of cell order) -- are queued
+//     per warp and deposited 32 at a time, one per lane, straight into the
+//     tile J, so a few such lanes do not stall the other lanes of their warp.
+constexpr int kGroups = 4;
+constexpr int kSlots = 54;
+constexpr int kQueue = 64;  // queued segments per warp
+
+// w (in units of 2^e_w) -> units of 2^e_tile, sh = e_w - e_tile, round half up
+__device__ __forceinline__ long long rescale(int w, int sh) {
+    return sh >= 0 ? (long long)w << sh : (sh > -62 ? ((long long)w + (1ll << (-sh - 1))) >> (-sh) : 0ll);
+}
+
 __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int sNHoles, sNFront, sNMove;
@@ -170,7 +187,10 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     __shared__ double sQ;
     __shared__ int sTileE;
     __shared__ float sInvQ;
-    __shared__ int sWarpAcc[kPushThreads / 32][96];
+    __shared__ int sWarpAcc[kPushThreads / 32][kGroups * kSlots];
+    __shared__ int sSlotNode[kSlots];
+    // queued segments: {stencil origin node, class bits, start x,y,z, end x,y,z}
+    __shared__ float4 sQueue[kPushThreads / 32][kQueue][2];
     const Grid &g = P.g;
     const int t = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -179,10 +199,10 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     const int i0 = ti * g.tx, l0 = tl * g.ty, k0 = tk * g.tz;
     const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
     const int nn = SX * SY * SZ;
-    // fixed-point tile J first (8-byte aligned), then the FP32 field tile
-    unsigned long long *sJ = (unsigned long long *)smem_raw;
-    float *sF = (float *)(sJ + 3 * nn);  // Ex Ey Ez Hx Hy Hz
-    int *sHoles = (int *)(sF + 6 * nn);
+    // FP32 field tile as yz-quads first (16-byte aligned), then the fixed-point tile J
+    float4 *sF = (float4 *)smem_raw;  // Ex Ey Ez Hx Hy Hz
+    unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);
+    int *sHoles = (int *)(sJ + 3 * nn);
     int *sFront = sHoles + kHoleMax;
     int *wacc = sWarpAcc[warp];
     if (threadIdx.x == 0) {
@@ -195,21 +215,35 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
         sTileE = e2 - 62;  // tile quantum 2^(e2-62)
         sInvQ = (float)ldexp(1.0, 62 - e2);
     }
-    for (int e = lane; e < 96; e += 32) wacc[e] = 0;
+    for (int e = lane; e < kGroups * kSlots; e += 32) wacc[e] = 0;
+    if (threadIdx.x < kSlots) {
+        // slot -> tile-local node offset from a cell's stencil origin (local index 0,0,0)
+        const int e = threadIdx.x;
+        int comp, a, b, c;
+        if (e < 18) { comp = 0; a = e / 9; b = (e / 3) % 3; c = e % 3; }
+        else if (e < 36) { comp = 1; a = (e - 18) / 6; b = ((e - 18) / 3) % 2; c = (e - 18) % 3; }
+        else { comp = 2; a = (e - 36) / 6; b = ((e - 36) / 2) % 3; c = (e - 36) % 2; }
+        sSlotNode[e] = comp * nn + ((2 + a) * SY + (2 + b)) * SZ + (2 + c);
+    }
 
     const float *const *E = (const float *const *)P.E;
     const float *const *H = (const float *const *)P.H;
+    const float *Fsrc[6] = {E[0], E[1], E[2], H[0], H[1], H[2]};
     for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
-        int c = idx % SZ, b = (idx / SZ) % SY, a = idx / (SZ * SY);
-        int gi = i0 + a, gl = l0 + b, gk = k0 + c;
-        bool in = gi < g.NX && gl < g.NY && gk < g.NZ;
-        size_t n = in ? g.node(gi, gl, gk) : 0;
-        sF[idx] = in ? E[0][n] : 0.f;
-        sF[nn + idx] = in ? E[1][n] : 0.f;
-        sF[2 * nn + idx] = in ? E[2][n] : 0.f;
-        sF[3 * nn + idx] = in ? H[0][n] : 0.f;
-        sF[4 * nn + idx] = in ? H[1][n] : 0.f;
-        sF[5 * nn + idx] = in ? H[2][n] : 0.f;
+        const int c = idx % SZ, b = (idx / SZ) % SY, a = idx / (SZ * SY);
+        const int gi = i0 + a, gl = l0 + b, gk = k0 + c;
+        // taps outside the staged tile or the field arrays are never read: 0
+        const bool in00 = gi < g.NX && gl < g.NY && gk < g.NZ;
+        const bool in01 = in00 && c + 1 < SZ && gk + 1 < g.NZ;
+        const bool in10 = in00 && b + 1 < SY && gl + 1 < g.NY;
+        const bool in11 = in01 && in10;
+        const size_t n = in00 ? g.node(gi, gl, gk) : 0;
+#pragma unroll
+        for (int f = 0; f < 6; f++) {
+            const float *F = Fsrc[f];
+            sF[f * nn + idx] = make_float4(in00 ? F[n] : 0.f, in01 ? F[n + 1] : 0.f, in10 ? F[n + g.pz] : 0.f,
+                                           in11 ? F[n + g.pz + 1] : 0.f);
+        }
         sJ[idx] = 0ull;
         sJ[nn + idx] = 0ull;
         sJ[2 * nn + idx] = 0ull;
@@ -217,11 +251,13 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     __syncthreads();
     const float inv_q = sInvQ;
     const int tile_e = sTileE;
+    const int slotA = sSlotNode[lane], slotB = lane < kSlots - 32 ? sSlotNode[32 + lane] : 0;
+    float4(*queue)[2] = sQueue[warp];
 
     const float ctx = (float)(g.tau / g.hx), cty = (float)(g.tau / g.hy), ctz = (float)(g.tau / g.hz);
     unsigned bad = 0;
     double kin = 0.0;
-    unsigned long long moved = 0;
+    unsigned long long moved = 0, unsorted = 0;
     OutMixed *outbox = (OutMixed *)P.outbox;
 
     for (int s = 0; s < P.nsp; s++) {
@@ -234,6 +270,24 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
         const float wx = (float)(S.m * g.hx / g.tau), wy = (float)(S.m * g.hy / g.tau), wz = (float)(S.m * g.hz / g.tau);
         if (threadIdx.x == 0) { sNHoles = 0; sNFront = 0; sNMove = 0; }
         __syncthreads();
+        int qn = 0;  // segments in this warp's queue (warp-uniform)
+        // deposit the queued segments [from, from + n), one per lane, into the tile J
+        auto drain_range = [&](int from, int n) {
+            if (lane < n) {
+                const float4 a = queue[from + lane][0], b = queue[from + lane][1];
+                const int cl = __float_as_int(a.y);
+                const int iv[3] = {2 + (cl & 1), 2 + ((cl >> 1) & 1), 2 + ((cl >> 2) & 1)};
+                const float qs[3] = {a.z, a.w, b.x}, qe[3] = {b.y, b.z, b.w};
+                float v[12];
+                pqr_mixed(iv, qs, qe, wx, wy, wz, v);
+                const int nb = __float_as_int(a.x) + (iv[0] * SY + iv[1]) * SZ + iv[2];
+#pragma unroll
+                for (int q = 0; q < 12; q++) fx_addf(&sJ[contrib_node(q, nb, nn, SY, SZ)], v[q], inv_q);
+            }
+            __syncwarp();
+        };
+        auto drain = [&](int n) { drain_range(0, n); };
+        auto drain_top32 = [&](int n) { drain_range(n - 32, 32); };
         // warp-synchronous loop: every lane of a warp runs the same iterations;
         // the next particle is loaded before the current one is processed
         const int stride = blockDim.x;
@@ -285,7 +339,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
                 float sv = pv + pw * bx - pu * bz;
                 float sw = pw + pu * by - pv * bx;
                 float q1 = bx * bx, q2 = by * by, q3 = bz * bz, q4 = bx * by, q5 = by * bz, q6 = bz * bx;
-                float rs = 1.f / (q1 + 1.f + q2 + q3);
+                float rs = __fdividef(1.f, q1 + 1.f + q2 + q3);
                 float pu1 = ((q1 + 1.f) * su + (q4 + bz) * sv + (q6 - by) * sw) * rs;
                 float pv1 = ((q4 - bz) * su + (q2 + 1.f) * sv + (q5 + bx) * sw) * rs;
                 float pw1 = ((q6 + by) * su + (q5 - bx) * sv + (q3 + 1.f) * sw) * rs;
@@ -295,9 +349,11 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
             }
             float p2 = pu * pu + pv * pv + pw * pw;
             float ig = rsqrtf(p2 + 1.f);
-            if (active && !(isfinite(pu) && isfinite(pv) && isfinite(pw))) bad |= ST_NAN;
-            // gamma - 1 = p^2 / (gamma + 1), accumulated in FP64
-            if (active) kin += M * (double)(p2 / (1.f / ig + 1.f));
+            // a non-finite momentum component makes p^2 non-finite
+            const bool finite = isfinite(p2);
+            if (active && !finite) bad |= ST_NAN;
+            // gamma - 1 = p^2 / (gamma + 1) = p^2 ig / (1 + ig), accumulated in FP64
+            if (active) kin += M * (double)__fdividef(p2 * ig, 1.f + ig);
             float xe[3] = {xs[0] + ctx * (ig * pu), xs[1] + cty * (ig * pv), xs[2] + ctz * (ig * pw)};
 
             // ---- CurrentToMesh (cell.h:1306-1422) in cell units
@@ -308,7 +364,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
             int i2[3];
 #pragma unroll
             for (int d = 0; d < 3; d++) i2[d] = 2 + (xe[d] >= 0.5f) + (xe[d] >= 1.5f) - (xe[d] < -0.5f);
-            bool dep = active && isfinite(xe[0]) && isfinite(xe[1]) && isfinite(xe[2]);
+            bool dep = active && finite;
             if (dep && (i2[0] < 2 || i2[0] > 3 || i2[1] < 2 || i2[1] > 3 || i2[2] < 2 || i2[2] > 3)) {
                 bad |= ST_STENCIL;
                 dep = false;
@@ -324,49 +380,85 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
             const int ew = max(exponent_above(wmax), -100);
             const float inv_qw = pow2f(22 - ew);
             const int sh = ew - 22 - tile_e;  // warp quantum / tile quantum = 2^sh
-            const unsigned am = __ballot_sync(FULL, dep);
-            const int lead = am ? __ffs(am) - 1 : 0;
-            const int lead_cell = __shfl_sync(FULL, cur.cell, lead);
-            const bool fast = dep && cur.cell == lead_cell;
-            if (dep) {
-                // two segments for every lane; the second has length 0 without a crossing
-                float x2[3], v[12];
-                split_point(i1, i2, xs, xe, x2);
-                auto deposit = [&](const int iv[3]) {
-                    const int cls = ((iv[0] - 2) << 2) | ((iv[1] - 2) << 1) | (iv[2] - 2);
-                    if (fast) {
-#pragma unroll
-                        for (int q = 0; q < 12; q++) {
-                            int w = __float_as_int(fmaf(v[q], inv_qw, 12582912.0f)) - 0x4B400000;  // round(v/q_w)
-                            if (w) atomicAdd(&wacc[cls * 12 + q], w);
-                        }
-                    } else {
-                        const int nb = n0 + (iv[0] * SY + iv[1]) * SZ + iv[2];
-#pragma unroll
-                        for (int q = 0; q < 12; q++) fx_addf(&sJ[contrib_node(q, nb, nn, SY, SZ)], v[q], inv_q);
-                    }
-                };
+            // one group per distinct cell among the depositing lanes
+            const unsigned same = __match_any_sync(FULL, dep ? cur.cell : -1);
+            const int leader = __ffs(same) - 1;
+            const unsigned leaders = __ballot_sync(FULL, dep && lane == leader);
+            const int grp = __popc(leaders & ((1u << leader) - 1));
+            const bool fast = dep && grp < kGroups;
+            unsorted += dep && !fast;
+            // the second zigzag segment exists only where a cell-centre plane is crossed
+            const bool cross = dep && (i2[0] != i1x || i2[1] != i1y || i2[2] != i1z);
+            float x2[3] = {xe[0], xe[1], xe[2]};
+            if (cross) split_point(i1, i2, xs, xe, x2);
+            if (fast) {
+                float v[12];
                 pqr_mixed(i1, xs, x2, wx, wy, wz, v);
-                deposit(i1);
-                pqr_mixed(i2, x2, xe, wx, wy, wz, v);
-                deposit(i2);
+                int *wb = wacc + grp * kSlots;
+                const int cx = i1x - 2, cy = i1y - 2, cz = i1z - 2;
+                const int bx = cx * 9 + cy * 3 + cz, by = 18 + cx * 6 + cy * 3 + cz, bz = 36 + cx * 6 + cy * 2 + cz;
+                const int off[12] = {bx, bx + 1, bx + 3, bx + 4, by, by + 1, by + 6, by + 7, bz, bz + 2, bz + 6, bz + 8};
+#pragma unroll
+                for (int q = 0; q < 12; q++) {
+                    int w = __float_as_int(fmaf(v[q], inv_qw, 12582912.0f)) - 0x4B400000;  // round(v/q_w)
+                    if (w) atomicAdd(&wb[off[q]], w);
+                }
+            }
+            // queue the other segments (warp-aggregated positions)
+            {
+                const bool t1 = dep && !fast, t2 = cross;
+                const unsigned b1 = __ballot_sync(FULL, t1), b2 = __ballot_sync(FULL, t2);
+                const unsigned lt = (1u << lane) - 1;
+                const int ntask = __popc(b1) + __popc(b2);
+                if (ntask) {
+                    if (qn + ntask > kQueue) {
+                        drain(qn);
+                        qn = 0;
+                    }
+                    int pos = qn + __popc(b1 & lt) + __popc(b2 & lt);
+                    const float n0f = __int_as_float(n0);
+                    if (t1) {
+                        queue[pos][0] = make_float4(n0f, __int_as_float((i1x - 2) | ((i1y - 2) << 1) | ((i1z - 2) << 2)),
+                                                    xs[0], xs[1]);
+                        queue[pos][1] = make_float4(xs[2], x2[0], x2[1], x2[2]);
+                        pos += t2;
+                    }
+                    if (t2) {
+                        queue[pos][0] = make_float4(n0f, __int_as_float((i2[0] - 2) | ((i2[1] - 2) << 1) | ((i2[2] - 2) << 2)),
+                                                    x2[0], x2[1]);
+                        queue[pos][1] = make_float4(x2[2], xe[0], xe[1], xe[2]);
+                    }
+                    qn += ntask;
+                    if (qn >= 32) {
+                        __syncwarp();
+                        drain_top32(qn);
+                        qn -= 32;
+                    }
+                }
             }
             __syncwarp();
-            if (am) {
-                // flush the per-warp sums of the lead cell into the tile J (exact: both
-                // quanta are powers of two, the tile bound keeps the result below 2^62)
-                int li, ll, lk;
-                g.cell_ijk(lead_cell, li, ll, lk);
-                const int ln0 = ((li - i0 - 2) * SY + (ll - l0 - 2)) * SZ + (lk - k0 - 2);
-                for (int e = lane; e < 96; e += 32) {
-                    int w = wacc[e];
+            // flush the per-warp group sums into the tile J (exact: both quanta are
+            // powers of two, the tile bound keeps the result below 2^62)
+            {
+                unsigned lm = leaders;
+                for (int gi = 0; gi < kGroups && lm; gi++) {
+                    const int ld = __ffs(lm) - 1;
+                    lm &= lm - 1;
+                    const int base = __shfl_sync(FULL, n0, ld);
+                    int *wg = wacc + gi * kSlots;
+                    int w = wg[lane];
                     if (w) {
-                        wacc[e] = 0;
-                        int cls = e / 12, q = e - cls * 12;
-                        int nb = ln0 + ((2 + (cls >> 2)) * SY + (2 + ((cls >> 1) & 1))) * SZ + 2 + (cls & 1);
-                        long long add = sh >= 0 ? (long long)w << sh
-                                        : (sh > -62 ? ((long long)w + (1ll << (-sh - 1))) >> (-sh) : 0ll);
-                        if (add) atomicAdd(&sJ[contrib_node(q, nb, nn, SY, SZ)], (unsigned long long)add);
+                        wg[lane] = 0;
+                        const long long add = rescale(w, sh);
+                        if (add) atomicAdd(&sJ[base + slotA], (unsigned long long)add);
+                    }
+                    if (lane < kSlots - 32) {
+                        w = wg[32 + lane];
+                        if (w) {
+                            wg[32 + lane] = 0;
+                            const long long add = rescale(w, sh);
+                            if (add) atomicAdd(&sJ[base + slotB], (unsigned long long)add);
+                        }
                     }
                 }
             }
@@ -388,7 +480,8 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
                 xe[d] = fminf(fmaxf(xe[d], 0.f), kOneBelow);
             }
             const int newcell = g.cell_of(ci[0], ci[1], ci[2]);
-            if (newcell == cur.cell || g.tile_of_cell(ci[0], ci[1], ci[2]) == t) {
+            if ((unsigned)(ci[0] - i0) < (unsigned)g.tx && (unsigned)(ci[1] - l0) < (unsigned)g.ty &&
+                (unsigned)(ci[2] - k0) < (unsigned)g.tz) {
                 S.cell[slot] = newcell;
                 S.ox[slot] = xe[0]; S.oy[slot] = xe[1]; S.oz[slot] = xe[2];
                 S.fx[slot] = pu; S.fy[slot] = pv; S.fz[slot] = pw;
@@ -410,6 +503,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
                 else bad |= ST_HOLES;
             }
         }
+        drain(qn);
         __syncthreads();
         const int L = sNHoles;
         if (L > 0 && L <= kHoleMax) {
@@ -454,6 +548,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     }
     if (bad) atomicOr(&P.st->flags, bad);
     if (moved) atomicAdd(&P.st->moved, moved);
+    if (unsorted) atomicAdd(&P.st->unsorted, unsorted);
 }
 
 }  // namespace
@@ -475,7 +570,13 @@ void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], dou
 
 size_t push_smem_mixed(const Grid &g) {
     size_t nn = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2);
-    return 6 * nn * sizeof(float) + 3 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
+    return 6 * nn * sizeof(float4) + 3 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
+}
+
+size_t push_smem_total_mixed(const Grid &g) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, k_push_mixed) != cudaSuccess) return (size_t)-1;
+    return push_smem_mixed(g) + a.sharedSizeBytes;
 }
 
 cudaError_t launch_push_mixed(const StepParams &p, cudaStream_t s) {

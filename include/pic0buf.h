@@ -256,6 +256,13 @@ const char *pic_error_string(int status);
  * [1] particles no cell accepted (dropped), [2] particles two or more cells
  * accepted (duplicated), [3] kernel launches of the step. */
 int pic_step_counters(pic_handle *h, int64_t *out4);
+/* Bin order of the FP32 form after the last step: [0] depositing particles
+ * that the push found outside the first few distinct cells of their warp
+ * (they take the slower per-particle deposit), [1] per-tile cell sorts the
+ * step ran (the bins are re-sorted by cell when [0] exceeds 2% of the
+ * particle slots).  Both are 0 in the FP64 form.  No counterpart in the
+ * reference, whose per-cell particle arrays are always grouped by cell. */
+int pic_sort_stats(pic_handle *h, int64_t *out2);
 /* Timings of the last pic_step in milliseconds (CUDA events on the handle's
  * stream): [0] B half step, [1] the push/deposit kernel alone, [2] migration
  * arrivals, [3] J fold + B completion + E update + E ghosts, [4] whole step. */
