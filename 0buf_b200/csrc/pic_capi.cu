@@ -286,19 +286,17 @@ int check_status(pic_handle *h) {
     return PIC_OK;
 }
 
-// FP32 form: sort every species' tile bins by cell (into the alternate
-// arrays, then swap) when the last push found more than 2% of its particles
-// outside their warp's lead cell -- the deposit's fast path needs sorted bins
+// FP32 form: sort a species' tile bins by cell (into the alternate arrays,
+// then swap) when the last push found more than 2% of its particle slots
+// outside the first few distinct cells of their warp -- the deposit sums a
+// warp's lanes per cell, which pays off when the bins are in cell order
 int maybe_sort(pic_handle *h) {
     h->sorts = 0;
     if (!h->mixed) return PIC_OK;
-    int64_t total = 0;
-    for (int s = 0; s < h->cfg.nspecies; s++) total += h->sp[s].cap_total;
-    if ((double)h->st_host->unsorted <= 0.02 * (double)total) return PIC_OK;
     for (int s = 0; s < h->cfg.nspecies; s++) {
         auto &S = h->sp[s];
-        if (!S.loaded || S.cap_total == 0) continue;
-        if (!S.alt_cell) continue;
+        if (!S.loaded || S.cap_total == 0 || !S.alt_cell) continue;
+        if ((double)h->st_host->unsorted[s] <= 0.02 * (double)S.cap_total) continue;
         SpeciesView D = S.v;
         D.cell = S.alt_cell;
         float **dp[6] = {&D.ox, &D.oy, &D.oz, &D.fx, &D.fy, &D.fz};
@@ -495,6 +493,7 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
     if ((e = cudaMalloc(&h->st, sizeof(DevStatus))) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(h->st, 0, sizeof(DevStatus), h->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaMallocHost(&h->st_host, sizeof(DevStatus))) != cudaSuccess) return fail(e);
+    memset(h->st_host, 0, sizeof(DevStatus));
     if ((e = cudaMalloc(&h->dred, 8 * sizeof(double))) != cudaSuccess) return fail(e);
     if ((e = cudaMallocHost(&h->hred, 8 * sizeof(double))) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&h->dcounts, (size_t)g.ncells() * sizeof(int))) != cudaSuccess) return fail(e);
@@ -927,7 +926,9 @@ int pic_step_counters(pic_handle *h, int64_t *out4) {
 
 int pic_sort_stats(pic_handle *h, int64_t *out2) {
     if (!h || !out2) return PIC_ERR_ARG;
-    out2[0] = h->mixed && h->st_host ? (int64_t)h->st_host->unsorted : 0;
+    out2[0] = 0;
+    if (h->mixed && h->st_host)
+        for (int s = 0; s < h->cfg.nspecies; s++) out2[0] += (int64_t)h->st_host->unsorted[s];
     out2[1] = h->sorts;
     return PIC_OK;
 }

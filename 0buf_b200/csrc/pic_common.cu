@@ -119,7 +119,7 @@ __global__ void k_scatter_f(Grid g, int mixed, int64_t n, const int *__restrict_
 // take one shared-memory atomic per cell (match.any), so runs of one cell
 // cost no conflicts, and the writes of a run are contiguous.  Entries whose
 // cell is not in the tile (never expected) go after the sorted ones.
-__global__ void __launch_bounds__(512) k_sort_tile_f(Grid g, SpeciesView S, SpeciesView D) {
+__global__ void __launch_bounds__(512, 2) k_sort_tile_f(Grid g, SpeciesView S, SpeciesView D) {
     extern __shared__ int s_off[];  // tile cells + 1
     __shared__ int s_wsum[32];
     __shared__ int s_carry;
@@ -176,11 +176,22 @@ __global__ void __launch_bounds__(512) k_sort_tile_f(Grid g, SpeciesView S, Spec
         if (threadIdx.x == 0) s_carry = carry + s_wsum[nw - 1];
         __syncthreads();
     }
-    // scatter: the first lane of each run of one cell reserves the run's slots
-    for (int j0 = 0; j0 < count; j0 += blockDim.x) {
-        const int j = j0 + threadIdx.x;
-        const int src = start + j;
-        const int c = j < count ? local(S.cell[src]) : -1;
+    // scatter: the first lane of each run of one cell reserves the run's slots;
+    // two entries per thread per pass, all loads issued before the writes
+    struct Ent {
+        int cell;
+        float v[6];
+    };
+    auto load_ent = [&](int j, int &c, Ent &e) {
+        c = j < count ? local(S.cell[start + j]) : -1;
+        if (c >= 0) {
+            const int src = start + j;
+            e.cell = S.cell[src];
+            e.v[0] = S.ox[src]; e.v[1] = S.oy[src]; e.v[2] = S.oz[src];
+            e.v[3] = S.fx[src]; e.v[4] = S.fy[src]; e.v[5] = S.fz[src];
+        }
+    };
+    auto place = [&](int c, const Ent &e) {
         const unsigned m = __match_any_sync(FULL, c);
         const int first = __ffs(m) - 1;
         int base = 0;
@@ -188,10 +199,18 @@ __global__ void __launch_bounds__(512) k_sort_tile_f(Grid g, SpeciesView S, Spec
         base = __shfl_sync(FULL, base, first);
         if (c >= 0) {
             const int dst = start + base + __popc(m & lt);
-            D.cell[dst] = S.cell[src];
-            D.ox[dst] = S.ox[src]; D.oy[dst] = S.oy[src]; D.oz[dst] = S.oz[src];
-            D.fx[dst] = S.fx[src]; D.fy[dst] = S.fy[src]; D.fz[dst] = S.fz[src];
+            D.cell[dst] = e.cell;
+            D.ox[dst] = e.v[0]; D.oy[dst] = e.v[1]; D.oz[dst] = e.v[2];
+            D.fx[dst] = e.v[3]; D.fy[dst] = e.v[4]; D.fz[dst] = e.v[5];
         }
+    };
+    for (int j0 = 0; j0 < count; j0 += 2 * blockDim.x) {
+        int c0, c1;
+        Ent e0, e1;
+        load_ent(j0 + threadIdx.x, c0, e0);
+        load_ent(j0 + blockDim.x + threadIdx.x, c1, e1);
+        place(c0, e0);
+        place(c1, e1);
     }
     // free slots of the tile stay marked empty in the new arrays
     for (int j = start + count + threadIdx.x; j < S.tile_start[t + 1]; j += blockDim.x) D.cell[j] = -1;

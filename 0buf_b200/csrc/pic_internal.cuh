@@ -45,8 +45,10 @@ struct DevStatus {
     unsigned long long dropped;
     unsigned long long duplicated;
     double kinetic;            // sum (m/q_m)(gamma-1) accumulated by the push
-    unsigned long long unsorted;  // mixed push: particles outside their warp's lead cell (bins out of cell order)
-    double pad1[2];
+    double pad1[3];
+    // mixed push, per species: depositing particles beyond the first kGroups
+    // distinct cells of their warp (bins out of cell order)
+    unsigned long long unsorted[kMaxSpecies];
 };
 
 struct Grid {

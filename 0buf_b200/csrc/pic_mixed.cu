@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     const float ctx = (float)(g.tau / g.hx), cty = (float)(g.tau / g.hy), ctz = (float)(g.tau / g.hz);
     unsigned bad = 0;
     double kin = 0.0;
-    unsigned long long moved = 0, unsorted = 0;
+    unsigned long long moved = 0;
     OutMixed *outbox = (OutMixed *)P.outbox;
 
     for (int s = 0; s < P.nsp; s++) {
@@ -270,6 +270,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
         const float wx = (float)(S.m * g.hx / g.tau), wy = (float)(S.m * g.hy / g.tau), wz = (float)(S.m * g.hz / g.tau);
         if (threadIdx.x == 0) { sNHoles = 0; sNFront = 0; sNMove = 0; }
         __syncthreads();
+        unsigned unsorted = 0;
         int qn = 0;  // segments in this warp's queue (warp-uniform)
         // deposit the queued segments [from, from + n), one per lane, into the tile J
         auto drain_range = [&](int from, int n) {
@@ -504,6 +505,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
             }
         }
         drain(qn);
+        if (unsorted) atomicAdd(&P.st->unsorted[s], (unsigned long long)unsorted);
         __syncthreads();
         const int L = sNHoles;
         if (L > 0 && L <= kHoleMax) {
@@ -548,7 +550,6 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     }
     if (bad) atomicOr(&P.st->flags, bad);
     if (moved) atomicAdd(&P.st->moved, moved);
-    if (unsorted) atomicAdd(&P.st->unsorted, unsorted);
 }
 
 }  // namespace
