@@ -93,6 +93,8 @@ SIGNATURES = {
     "pic_energy": (C.c_int, [H, D]),
     "pic_energy_reference": (C.c_int, [H, D]),
     "pic_charge_density": (C.c_int, [H, D]),
+    "pic_gauss_residual": (C.c_int, [H, D]),
+    "pic_gauss_check": (C.c_int, [H, C.c_int, D]),
     "pic_sync": (C.c_int, [H]),
     "pic_last_status": (C.c_int, [H]),
     "pic_last_error_string": (C.c_char_p, [H]),

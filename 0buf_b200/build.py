@@ -35,6 +35,7 @@ UNITS = {
     "pic_arch.cu": [],
     "pic_mixed.cu": [],
     "pic_noalloc.cu": [],
+    "pic_diag.cu": ["-fmad=false"],
     "pic_adjoint.cu": ["-fmad=false"],
     "pic_adjoint_mixed.cu": [],
 }

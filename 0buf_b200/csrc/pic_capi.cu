@@ -517,6 +517,9 @@ int pic_destroy(pic_handle *h) {
     if (h->dred) cudaFree(h->dred);
     if (h->hred) cudaFreeHost(h->hred);
     if (h->dcounts) cudaFree(h->dcounts);
+    double *diag[3] = {h->rho, h->gauss, h->gauss0};
+    for (double *d : diag)
+        if (d) cudaFree(d);
     for (int i = 0; i < 6; i++)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -883,11 +886,6 @@ int pic_energy_reference(pic_handle *h, double *out) {
     CK(cudaStreamSynchronize(h->stream), "sync");
     *out = h->hred[2];
     return PIC_OK;
-}
-
-int pic_charge_density(pic_handle *h, double *rho_host) {
-    (void)rho_host;
-    return set_err(h, PIC_ERR_NOT_BUILT, "charge density is not built in this version");
 }
 
 int pic_sync(pic_handle *h) {

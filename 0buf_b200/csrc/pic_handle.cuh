@@ -49,6 +49,10 @@ struct pic_handle {
     int timed;
     int kin_valid;  // st->kinetic holds the kinetic energy of the current momenta
     pic::AdjState *adj;
+    // charge-conservation diagnostic (pic_diag.cu), allocated on first use:
+    // rho, the Gauss residual G = div E - rho and its stored baseline
+    double *rho, *gauss, *gauss0;
+    int gauss_has_base;
 };
 
 namespace pic_host {
@@ -57,6 +61,8 @@ int set_err(pic_handle *h, int code, const char *msg);
 int cuda_err(pic_handle *h, cudaError_t e, const char *where);
 int set_device(pic_handle *h);
 int need_particles(pic_handle *h);
+// kernel parameters of the current state (species views, fields, outbox, status)
+pic::StepParams make_params(pic_handle *h);
 // flat device list of one species (packed cell, FP64 global positions and
 // momenta; cell < 0 = rejected) -> bins of species s
 int build_bins(pic_handle *h, int s, int64_t n, int *cell, const double *x, const double *y, const double *z,

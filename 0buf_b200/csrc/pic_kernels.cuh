@@ -59,6 +59,12 @@ cudaError_t init_species_bins(const Grid &g, int mixed, SpeciesView sv, int spec
 cudaError_t field_energy(const Grid &g, int mixed, const void *const E[3], const void *const H[3], double *out3,
                          cudaStream_t s);
 cudaError_t kinetic_energy(const StepParams &p, double *out, cudaStream_t s);
+// charge-conservation diagnostic (pic_diag.cu, FP64): rho on the cell-centre
+// nodes, folded; G = div E - rho on interior nodes with reductions
+// red[0] max |G - G0|, red[1] max |rho|, red[2] sum (G - G0)^2, red[3] max |G0|
+cudaError_t charge_density(const StepParams &p, double *rho, cudaStream_t s);
+cudaError_t gauss_residual(const Grid &g, int mixed, const void *const E[3], const double *rho, double *G, double *G0,
+                           int set_baseline, double *red, cudaStream_t s);
 // pitched device <-> dense reference-layout buffer (FP64 on the dense side)
 cudaError_t pitched_to_dense(const Grid &g, const void *src, int is_float, double *dst, cudaStream_t s);
 cudaError_t dense_to_pitched(const Grid &g, const double *src, void *dst, int is_float, cudaStream_t s);

@@ -174,6 +174,24 @@ class PicSimulation:
         self._ck(self.lib.pic_energy(self.h, dptr(e)), "pic_energy")
         return e
 
+    def charge_density(self) -> np.ndarray:
+        """rho on the cell-centre nodes (linear weights, folded), reference layout."""
+        a = np.zeros(int(np.prod(self.shape)))
+        self._ck(self.lib.pic_charge_density(self.h, dptr(a)), "pic_charge_density")
+        return a
+
+    def gauss_residual(self) -> np.ndarray:
+        """G = div E - rho on the interior nodes (0 on ghosts), reference layout."""
+        a = np.zeros(int(np.prod(self.shape)))
+        self._ck(self.lib.pic_gauss_residual(self.h, dptr(a)), "pic_gauss_residual")
+        return a
+
+    def gauss_check(self, set_baseline: bool = False) -> np.ndarray:
+        """[max |G - G0|, max |rho|, rms(G - G0), max |G0|]; set_baseline stores G as G0."""
+        out = np.zeros(4)
+        self._ck(self.lib.pic_gauss_check(self.h, int(bool(set_baseline)), dptr(out)), "pic_gauss_check")
+        return out
+
     def energy_reference(self) -> float:
         e = np.zeros(1)
         self._ck(self.lib.pic_energy_reference(self.h, dptr(e)), "pic_energy_reference")

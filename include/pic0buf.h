@@ -176,9 +176,24 @@ int pic_get_particles(pic_handle *h, int species, int64_t cap, double *x, double
  * wrap_kernel.cu:14-36), which pic_energy_reference returns. */
 int pic_energy(pic_handle *h, double *out4);
 int pic_energy_reference(pic_handle *h, double *out);
-/* Charge-conservation residual: max |div E - div E(t0) + (rho - rho(t0))|
- * style check -- see pic_charge_residual in the implementation notes. */
+/* Charge conservation in FP64 (no counterpart in the reference, which has no
+ * charge density).  rho[N] = sum over particles of m times the linear
+ * (cloud-in-cell) weights on the nodes at cell centres -- array index N sits
+ * at (N - 1/2) h per axis -- folded across the periodic boundaries like the
+ * current (periodicCurrentElement, kernels.cu:1124-1146).  With the zigzag
+ * deposit (CurrentToMesh, cell.h:1306-1422) and the E update (emeElement,
+ * kernels.cu:1091-1102) the Gauss residual
+ *   G[N] = sum_a (E_a[N] - E_a[N - e_a]) / h_a - rho[N]   (interior nodes)
+ * stays what it was at the start, up to rounding.
+ * pic_charge_density: rho in the reference layout (NULL: compute only).
+ * pic_gauss_residual: G in the reference layout (0 on ghost nodes).
+ * pic_gauss_check: computes G on the device; with set_baseline != 0 stores it
+ *   as the baseline G0.  out4 = [max |G - G0|, max |rho|, rms over interior
+ *   nodes of (G - G0), max |G0|].  Without a stored baseline and
+ *   set_baseline = 0 it returns PIC_ERR_ARG. */
 int pic_charge_density(pic_handle *h, double *rho_host);
+int pic_gauss_residual(pic_handle *h, double *g_host);
+int pic_gauss_check(pic_handle *h, int set_baseline, double *out4);
 
 /* Differentiable run (no counterpart in the reference, which has no
  * gradients).  pic_forward advances the state by `steps` time steps with the

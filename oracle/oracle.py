@@ -192,3 +192,59 @@ class RefSim(_Sim):
     @classmethod
     def available(cls) -> bool:
         return os.path.exists(cls.libpath)
+
+
+# ---------------------------------------------------------------------------
+# Charge conservation (no counterpart in the reference, which has no charge
+# density).  The zigzag deposit puts its nodes at cell centres: pqr
+# (cell.h:1511-1693) weights node index iv of a particle's 5-node stencil by
+# its distance to iv - 2.5 cells from the cell origin, so array node N sits at
+# (N - 1/2) h per axis.  With rho assigned by the same linear weights and
+# folded like the current (periodicCurrentElement, kernels.cu:1124-1146), and
+# the E update's backward-difference divergence (emeElement,
+# kernels.cu:1091-1102), G = div E - rho on the interior nodes is constant.
+
+def charge_density(x, y, z, m, cells, h):
+    """rho on the (nx+2)(ny+2)(nz+2) nodes, reference layout (flat); x, y, z
+    global positions, m the signed charge weight per particle (array or
+    scalar), h the cell sizes (3,)."""
+    cells = tuple(int(c) for c in cells)
+    shape = tuple(c + 2 for c in cells)
+    r = np.zeros(shape)
+    xc = np.stack([np.asarray(x) / h[0], np.asarray(y) / h[1], np.asarray(z) / h[2]], 1)
+    cell = np.floor(xc).astype(np.int64)
+    f = xc - cell
+    up = (f >= 0.5).astype(np.int64)
+    N0 = cell + up
+    w1 = f + 0.5 - up
+    m = np.broadcast_to(np.asarray(m, dtype=np.float64), (xc.shape[0],))
+    for a in (0, 1):
+        for b in (0, 1):
+            for c in (0, 1):
+                w = (w1[:, 0] if a else 1 - w1[:, 0]) * (w1[:, 1] if b else 1 - w1[:, 1]) * \
+                    (w1[:, 2] if c else 1 - w1[:, 2])
+                np.add.at(r, (N0[:, 0] + a, N0[:, 1] + b, N0[:, 2] + c), m * w)
+    for ax in range(3):
+        n = cells[ax]
+        r = np.moveaxis(r, ax, 0)
+        r[n] += r[0]
+        r[1] += r[n + 1]
+        r[0] = r[n]
+        r[n + 1] = r[1]
+        r = np.moveaxis(r, 0, ax)
+    return r.ravel()
+
+
+def gauss_residual(Ex, Ey, Ez, rho, cells, h):
+    """G = div E - rho on the interior nodes (backward differences), 0 on the
+    ghost nodes; flat reference layout."""
+    cells = tuple(int(c) for c in cells)
+    shape = tuple(c + 2 for c in cells)
+    E = [np.asarray(a, dtype=np.float64).reshape(shape) for a in (Ex, Ey, Ez)]
+    r = np.asarray(rho, dtype=np.float64).reshape(shape)
+    nx, ny, nz = cells
+    I, J, K = slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1)
+    G = np.zeros(shape)
+    G[I, J, K] = ((E[0][I, J, K] - E[0][0:nx, J, K]) / h[0] + (E[1][I, J, K] - E[1][I, 0:ny, K]) / h[1] +
+                  (E[2][I, J, K] - E[2][I, J, 0:nz]) / h[2] - r[I, J, K])
+    return G.ravel()

@@ -133,3 +133,39 @@ def test_oracle_reports_cfl_violation(oracle_mod):
     sim.add_particles(1, one(0.19), one(0.15), one(0.15), one(40.0), one(0.0), one(0.0), -0.1, -1.0)
     rcs = [sim.substep(s) for s in oracle_mod.SUBSTEPS[:5]]
     assert rcs[4] == -3
+
+
+def test_gauss_law_conserved_by_reference_outputs(oracle_mod):
+    """The charge assignment of oracle.charge_density (linear weights on the
+    cell-centre nodes, folded like the current) makes G = div E - rho a
+    constant of the reference's own step: G from the fixture's inputs equals G
+    after steps 1 and 4 of the reference (random initial E, all species)."""
+    d = np.load(os.path.join(GOLDEN, "ref_small.npz"))
+    cells = tuple(int(c) for c in d["cells"])
+    h = (float(d["h"]),) * 3
+    m_of = np.array([float(d[f"in_s{s}_m"]) for s in range(3)])
+    xs = [np.concatenate([d[f"in_s{s}_{k}"] for s in range(3)]) for k in ("x", "y", "z")]
+    ms = np.concatenate([np.full(d["in_s0_x"].size, m_of[0]), np.full(d["in_s1_x"].size, m_of[1]),
+                         np.full(d["in_s2_x"].size, m_of[2])])
+    rho0 = oracle_mod.charge_density(*xs, ms, cells, h)
+    G0 = oracle_mod.gauss_residual(d["in_Ex"], d["in_Ey"], d["in_Ez"], rho0, cells, h)
+    scale = np.abs(rho0).max()
+    assert scale > 0 and np.abs(G0).max() > 0.1 * scale
+    for st in (1, 4):
+        P = d[f"step{st}_particles"]
+        m = m_of[P[:, 1].astype(int)]
+        rho = oracle_mod.charge_density(P[:, 2], P[:, 3], P[:, 4], m, cells, h)
+        G = oracle_mod.gauss_residual(d[f"step{st}_Ex"], d[f"step{st}_Ey"], d[f"step{st}_Ez"], rho, cells, h)
+        assert np.abs(G - G0).max() < 1e-12 * np.abs(G0).max(), st
+        assert np.abs(rho - rho0).max() > 1e-6 * scale  # the charge did move
+
+
+def test_charge_density_totals(oracle_mod):
+    """rho on the interior nodes sums to the total charge (the fold keeps it)."""
+    rng = np.random.default_rng(5)
+    cells, h = (6, 5, 4), (0.1, 0.2, 0.3)
+    L = [c * hh for c, hh in zip(cells, h)]
+    x, y, z = (rng.uniform(0, l, 500) for l in L)
+    m = rng.normal(0, 1, 500)
+    r = oracle_mod.charge_density(x, y, z, m, cells, h).reshape(tuple(c + 2 for c in cells))
+    np.testing.assert_allclose(r[1:-1, 1:-1, 1:-1].sum(), m.sum(), rtol=1e-12, atol=1e-12)
