@@ -95,6 +95,7 @@ SIGNATURES = {
     "pic_charge_density": (C.c_int, [H, D]),
     "pic_gauss_residual": (C.c_int, [H, D]),
     "pic_gauss_check": (C.c_int, [H, C.c_int, D]),
+    "pic_momentum": (C.c_int, [H, D]),
     "pic_sync": (C.c_int, [H]),
     "pic_last_status": (C.c_int, [H]),
     "pic_last_error_string": (C.c_char_p, [H]),

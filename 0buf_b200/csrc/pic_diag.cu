@@ -163,7 +163,46 @@ __global__ void k_gauss(Grid g, const T *__restrict__ Ex, const T *__restrict__ 
     }
 }
 
+// total mechanical momentum per species, sum over particles of (m/q_m) p, in
+// FP64: one block per (tile, species), out[3 s + a]
+__global__ void k_momentum(StepParams P, double *out) {
+    __shared__ double red[3][32];
+    const SpeciesView &S = P.sp[blockIdx.y];
+    const int t = blockIdx.x;
+    const int start = S.tile_start[t], n = S.tile_count[t];
+    const double M = S.m / S.q_m;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int slot = start + j;
+        if (S.cell[slot] < 0) continue;
+        if (P.mixed) {
+            acc[0] += M * (double)S.fx[slot]; acc[1] += M * (double)S.fy[slot]; acc[2] += M * (double)S.fz[slot];
+        } else {
+            acc[0] += M * S.px[slot]; acc[1] += M * S.py[slot]; acc[2] += M * S.pz[slot];
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int a = 0; a < 3; a++) {
+        double v = acc[a];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[a][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double tot = 0.0;
+        for (int i = 0; i < nw; i++) tot += red[threadIdx.x][i];
+        atomicAdd(&out[3 * blockIdx.y + threadIdx.x], tot);
+    }
+}
+
 }  // namespace
+
+cudaError_t momentum(const StepParams &p, double *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, 3 * p.nsp * sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    k_momentum<<<dim3(p.g.ntiles, p.nsp), 256, 0, s>>>(p, out);
+    return cudaGetLastError();
+}
 
 cudaError_t charge_density(const StepParams &p, double *rho, cudaStream_t s) {
     const Grid &g = p.g;
@@ -266,6 +305,20 @@ int pic_gauss_residual(pic_handle *h, double *g_host) {
         CK(cudaMemcpyAsync(g_host, h->dense, h->g.nodes_ref() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
            "D2H residual");
     }
+    CK(cudaStreamSynchronize(h->stream), "sync");
+    return PIC_OK;
+}
+
+int pic_momentum(pic_handle *h, double *out) {
+    if (!h || !out) return PIC_ERR_ARG;
+    int rc = set_device(h);
+    if (rc) return rc;
+    if ((rc = need_particles(h))) return rc;
+    if ((rc = ensure_diag(h))) return rc;
+    StepParams p = make_params(h);
+    // the rho array is free scratch between diagnostic calls
+    CK(momentum(p, h->rho, h->stream), "momentum");
+    CK(cudaMemcpyAsync(out, h->rho, 3 * p.nsp * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "D2H momentum");
     CK(cudaStreamSynchronize(h->stream), "sync");
     return PIC_OK;
 }

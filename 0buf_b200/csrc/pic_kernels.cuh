@@ -63,6 +63,8 @@ cudaError_t kinetic_energy(const StepParams &p, double *out, cudaStream_t s);
 // nodes, folded; G = div E - rho on interior nodes with reductions
 // red[0] max |G - G0|, red[1] max |rho|, red[2] sum (G - G0)^2, red[3] max |G0|
 cudaError_t charge_density(const StepParams &p, double *rho, cudaStream_t s);
+// total mechanical momentum sum (m/q_m) p per species into out[3 s + a] (FP64)
+cudaError_t momentum(const StepParams &p, double *out, cudaStream_t s);
 cudaError_t gauss_residual(const Grid &g, int mixed, const void *const E[3], const double *rho, double *G, double *G0,
                            int set_baseline, double *red, cudaStream_t s);
 // pitched device <-> dense reference-layout buffer (FP64 on the dense side)

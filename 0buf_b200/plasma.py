@@ -186,6 +186,12 @@ class PicSimulation:
         self._ck(self.lib.pic_gauss_residual(self.h, dptr(a)), "pic_gauss_residual")
         return a
 
+    def momentum(self) -> np.ndarray:
+        """(nspecies, 3) total mechanical momentum sum (m/q_m) p per species, FP64."""
+        out = np.zeros(3 * self.nspecies)
+        self._ck(self.lib.pic_momentum(self.h, dptr(out)), "pic_momentum")
+        return out.reshape(self.nspecies, 3)
+
     def gauss_check(self, set_baseline: bool = False) -> np.ndarray:
         """[max |G - G0|, max |rho|, rms(G - G0), max |G0|]; set_baseline stores G as G0."""
         out = np.zeros(4)

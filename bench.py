@@ -220,6 +220,7 @@ def run_ours(args, dist):
 
     sim = make_sim(pkg, cfg, form, dev, seed_base)
     n_local = sim.num_particles()
+    sim.gauss_check(set_baseline=True)
     for w in range(W):
         sim.step(w + 1)
     dist.barrier()
@@ -236,6 +237,7 @@ def run_ours(args, dist):
     yee_ms = statistics.mean(phases["b_half"]) + statistics.mean(phases["fields2"])
     layout = sim.layout()
     energy_last = sim.energy().tolist()
+    state_last = {"energy": sim.energy(), "momentum": sim.momentum(), "gauss": sim.gauss_check()}
     sim.close()
     del sim
 
@@ -272,21 +274,30 @@ def run_ours(args, dist):
     if clocks:
         out["clocks"] = clocks
 
-    # FP64 plain form at the same configuration (N=1 only): the >= 2x claim
+    # FP64 plain form at the same configuration (N=1 only): the >= 2x claim,
+    # and the FP32 form's error against this FP64 run from the same seed after
+    # the same W + K steps (untimed steps fill up to W + K)
     if dist.world == 1 and not args.no_plain and form == "fp32":
         simp = make_sim(pkg, cfg, "fp64", dev, seed_base)
+        simp.gauss_check(set_baseline=True)
         for w in range(2):
             simp.step(w + 1)
         Kp = max(3, K // 2)
         ms_p, ph_p, _ = timed_steps(simp, Kp, torch)
+        for k in range(2 + Kp, W + K):
+            simp.step(k + 1)
         vp = n_local * Kp / (ms_p / 1e3)
         pp = statistics.mean(ph_p["push"])
         out["plain_fp64"] = {"value": round(vp, 1), "ms_per_step": round(ms_p / Kp, 4), "steps": Kp,
                              "push_ms": round(pp, 4),
                              "push_achieved_gbs": round(104 * n_local / (pp / 1e3) / 1e9, 1),
                              "mixed_over_plain": round(value / vp, 3)}
+        ref = {"energy": simp.energy(), "momentum": simp.momentum(), "gauss": simp.gauss_check()}
+        out["accuracy"] = accuracy_vs_fp64(state_last, ref, W + K)
         simp.close()
         del simp
+        if args.accuracy_steps > 0:
+            out["accuracy_long"] = accuracy_history(pkg, cfg, dev, seed_base, args.accuracy_steps)
 
     if not args.no_e2e:
         out["e2e"] = run_e2e(args, dist, pkg, cfg, form, torch, n_local)
@@ -294,6 +305,49 @@ def run_ours(args, dist):
         out["adjoint"] = run_adjoint(args, pkg, dev)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+def accuracy_vs_fp64(s32, s64, steps):
+    """FP32-form errors against the FP64 form after the same steps from the same
+    seed: energies [E field, B field, kinetic, total] relative to the FP64
+    total; total momentum per species relative to the largest per-species
+    FP64 momentum |(m/q_m) sum p|; Gauss residual drift max |G - G0| over max |rho|."""
+    import numpy as np
+    e32, e64 = np.asarray(s32["energy"]), np.asarray(s64["energy"])
+    p32, p64 = np.asarray(s32["momentum"]), np.asarray(s64["momentum"])
+    tot = abs(e64[3])
+    pscale = max(float(np.linalg.norm(p64, axis=1).max()), 1e-300)
+    return {"steps": steps,
+            "total_energy_rel_err": float(f"{abs(e32[3] - e64[3]) / tot:.3e}"),
+            "field_E_energy_rel_err": float(f"{abs(e32[0] - e64[0]) / abs(e64[0]):.3e}"),
+            "field_B_energy_rel_err": float(f"{abs(e32[1] - e64[1]) / max(abs(e64[1]), 1e-300):.3e}"),
+            "kinetic_energy_rel_err": float(f"{abs(e32[2] - e64[2]) / abs(e64[2]):.3e}"),
+            "momentum_rel_err": float(f"{float(np.linalg.norm(p32 - p64, axis=1).max()) / pscale:.3e}"),
+            "gauss_drift_fp32": float(f"{s32['gauss'][0] / s32['gauss'][1]:.3e}"),
+            "gauss_drift_fp64": float(f"{s64['gauss'][0] / s64['gauss'][1]:.3e}"),
+            "note": "energies relative to the FP64 value (total energy: of the FP64 total); gauss drift = "
+                    "max |G - G0| / max |rho|, G = div E - rho in FP64 on the device"}
+
+
+def accuracy_history(pkg, cfg, dev, seed_base, steps):
+    """Both forms from the same seed for `steps` steps, energies every step:
+    the largest relative total-energy and field-energy errors over the run,
+    and the final momentum and Gauss-residual errors."""
+    import numpy as np
+    hist, final = {}, {}
+    for form in ("fp32", "fp64"):
+        sim = make_sim(pkg, cfg, form, dev, seed_base)
+        sim.gauss_check(set_baseline=True)
+        hist[form] = sim.run(steps, energies=True)
+        final[form] = {"energy": sim.energy(), "momentum": sim.momentum(), "gauss": sim.gauss_check()}
+        sim.close()
+    h32, h64 = hist["fp32"], hist["fp64"]
+    out = accuracy_vs_fp64(final["fp32"], final["fp64"], steps)
+    out["max_over_steps_total_energy_rel_err"] = float(f"{np.max(np.abs(h32[:, 3] - h64[:, 3]) / np.abs(h64[:, 3])):.3e}")
+    out["max_over_steps_field_E_energy_rel_err"] = float(
+        f"{np.max(np.abs(h32[:, 0] - h64[:, 0]) / np.maximum(np.abs(h64[:, 0]), 1e-300)):.3e}")
+    out["total_energy_fp64_first_last"] = [float(h64[0, 3]), float(h64[-1, 3])]
     return out
 
 
@@ -547,6 +601,8 @@ def main():
     ap.add_argument("--adjoint-dirs", type=int, default=4,
                     help="random single-particle directions of the finite-difference check")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--accuracy-steps", type=int, default=0,
+                    help="also run both forms this many steps with energies every step (FP32 error history)")
     ap.add_argument("--reference-inner", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3:

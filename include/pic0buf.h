@@ -194,6 +194,10 @@ int pic_energy_reference(pic_handle *h, double *out);
 int pic_charge_density(pic_handle *h, double *rho_host);
 int pic_gauss_residual(pic_handle *h, double *g_host);
 int pic_gauss_check(pic_handle *h, int set_baseline, double *out4);
+/* Total mechanical momentum of each species in FP64: out[3 s + a] = sum over
+ * its particles of (m / q_m) p_a (p = gamma v, c = 1).  No counterpart in the
+ * reference; used to state the FP32 form's momentum error. */
+int pic_momentum(pic_handle *h, double *out);
 
 /* Differentiable run (no counterpart in the reference, which has no
  * gradients).  pic_forward advances the state by `steps` time steps with the

@@ -103,3 +103,16 @@ def test_gauss_check_needs_baseline(pkg):
         sim.init_species(0, 2, (0.0, 0.0, 0.0), 0.01, seed=1)
         with pytest.raises(pkg.PicError):
             sim.gauss_check()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_momentum_matches_particles(pkg, precision):
+    d, sim, cells, h = golden_sim(pkg, precision)
+    with sim:
+        sim.step(1)
+        P = sim.momentum()
+        for s in range(3):
+            p = sim.particles(s)
+            M = sim.cfg.species[s].m / sim.cfg.species[s].q_m
+            ref = M * np.array([p["px"].sum(), p["py"].sum(), p["pz"].sum()])
+            np.testing.assert_allclose(P[s], ref, rtol=1e-12, atol=1e-15 * abs(M) * p["px"].size)
