@@ -56,6 +56,11 @@ class PicGrads(C.Structure):
                 ("d_p0", C.c_void_p), ("reserved", C.c_double * 4)]
 
 
+class PicProfile(C.Structure):
+    _fields_ = [("ppc_mean", C.c_double), ("cos_amp", C.c_double), ("bump_peak", C.c_double),
+                ("bump_sigma", C.c_double), ("bump_centre", C.c_double * 3), ("count_seed", C.c_uint64)]
+
+
 D = C.POINTER(C.c_double)
 F = C.POINTER(C.c_float)
 I32 = C.POINTER(C.c_int)
@@ -96,6 +101,8 @@ SIGNATURES = {
     "pic_gauss_residual": (C.c_int, [H, D]),
     "pic_gauss_check": (C.c_int, [H, C.c_int, D]),
     "pic_momentum": (C.c_int, [H, D]),
+    "pic_profile_counts": (C.c_int, [C.c_int] * 3 + [C.POINTER(PicProfile), I32, I64]),
+    "pic_init_species_profile": (C.c_int, [H, C.c_int, C.POINTER(PicProfile)] + [C.c_double] * 4 + [C.c_uint64]),
     "pic_sync": (C.c_int, [H]),
     "pic_last_status": (C.c_int, [H]),
     "pic_last_error_string": (C.c_char_p, [H]),

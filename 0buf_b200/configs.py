@@ -30,8 +30,36 @@ CONFIGS = {
     # adjoint / differentiation case
     "c3": dict(cells=(128, 32, 32), h=0.1, tau=0.02, steps=300, ppc=32, precision="fp64"),
     # stress: non-uniform electron density, hot electrons, dt = 0.05
-    "c4": dict(cells=(256, 64, 64), h=0.1, tau=0.05, steps=500, ppc=64, precision="fp32"),
+    "c4": dict(cells=(256, 64, 64), h=0.1, tau=0.05, steps=500, ppc=64, precision="fp32", species=None),
 }
+
+
+# stress configuration c4: background electrons with density
+# (1 + 0.5 cos(2 pi x / Lx)) x (1 + 7 exp(-d^2 / (2 (4 cells)^2))) -- a bump of
+# 8x the local background at the box centre -- normalised to a mean of ppc
+# particles per cell; ions with the same per-cell counts (same profile and
+# count seed: neutral cell by cell up to the beam); hot electrons vth = 0.1;
+# beam uniform as in c0
+C4_PROFILE = dict(cos_amp=0.5, bump_peak=8.0, bump_sigma=4.0, bump_centre=(-1.0, -1.0, -1.0), count_seed=4)
+SPECIES_STRESS = [
+    dict(SPECIES_BEAM_PLASMA[0], profile=C4_PROFILE),
+    dict(SPECIES_BEAM_PLASMA[1], vth=0.1, profile=C4_PROFILE),
+    dict(SPECIES_BEAM_PLASMA[2]),
+]
+
+
+CONFIGS["c4"]["species"] = SPECIES_STRESS
+
+
+def init_config_species(sim, cfg: dict, seed_base: int = 0):
+    """Generate the species of a configuration on the device (uniform, or the
+    stress profile for c4)."""
+    ppc = cfg["ppc"]
+    for i, s in enumerate(cfg.get("species", SPECIES_BEAM_PLASMA)):
+        if "profile" in s:
+            sim.init_species_profile(i, dict(s["profile"], ppc_mean=ppc), s["drift"], s["vth"], seed_base + i)
+        else:
+            sim.init_species(i, ppc, s["drift"], s["vth"], seed_base + i)
 
 
 def charge_weight(q_m: float, density: float, ppc: int) -> float:

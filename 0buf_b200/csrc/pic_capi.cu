@@ -651,6 +651,86 @@ int pic_init_species_device(pic_handle *h, int species, int ppc, double drift_x,
     return ensure_outbox(h);
 }
 
+int pic_profile_counts(int nx, int ny, int nz, const pic_profile *prof, int32_t *counts, int64_t *total) {
+    if (nx < 1 || ny < 1 || nz < 1 || !prof || !counts) return PIC_ERR_ARG;
+    if (!(prof->ppc_mean >= 0) || !(prof->bump_peak > 0) || (prof->bump_peak != 1.0 && !(prof->bump_sigma > 0)))
+        return PIC_ERR_ARG;
+    const int64_t nc = (int64_t)nx * ny * nz;
+    double c0[3] = {prof->bump_centre[0], prof->bump_centre[1], prof->bump_centre[2]};
+    if (c0[0] < 0 || c0[1] < 0 || c0[2] < 0) { c0[0] = 0.5 * nx; c0[1] = 0.5 * ny; c0[2] = 0.5 * nz; }
+    const double two_pi = 6.283185307179586;
+    auto f_of = [&](int i, int l, int k) {
+        double a = 1.0 + prof->cos_amp * cos(two_pi * (i + 0.5) / nx);
+        double dxc = i + 0.5 - c0[0], dyc = l + 0.5 - c0[1], dzc = k + 0.5 - c0[2];
+        double b = prof->bump_peak == 1.0 ? 1.0
+                   : 1.0 + (prof->bump_peak - 1.0) *
+                               exp(-(dxc * dxc + dyc * dyc + dzc * dzc) / (2.0 * prof->bump_sigma * prof->bump_sigma));
+        return a * b;
+    };
+    double sum = 0.0;
+    for (int i = 0; i < nx; i++)
+        for (int l = 0; l < ny; l++)
+            for (int k = 0; k < nz; k++) sum += f_of(i, l, k);
+    if (!(sum > 0)) return PIC_ERR_ARG;
+    const double scale = prof->ppc_mean * (double)nc / sum;
+    int64_t acc = 0;
+    for (int i = 0; i < nx; i++)
+        for (int l = 0; l < ny; l++)
+            for (int k = 0; k < nz; k++) {
+                const int64_t c = ((int64_t)i * ny + l) * nz + k;
+                const double v = scale * f_of(i, l, k);
+                const double fl = floor(v);
+                const int n = (int)fl + (rng_uniform(prof->count_seed, -1, c, 0, 31) < v - fl ? 1 : 0);
+                counts[c] = n;
+                acc += n;
+            }
+    if (total) *total = acc;
+    return PIC_OK;
+}
+
+int pic_init_species_profile(pic_handle *h, int species, const pic_profile *prof, double drift_x, double drift_y,
+                             double drift_z, double vth, uint64_t seed) {
+    if (!h || species < 0 || species >= h->cfg.nspecies || !prof) return set_err(h, PIC_ERR_ARG, "bad argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    const Grid &g = h->g;
+    const int nc = g.ncells();
+    std::vector<int> cnt(nc), first(nc), tcount(g.ntiles, 0);
+    int64_t total = 0;
+    if (pic_profile_counts(g.nx, g.ny, g.nz, prof, cnt.data(), &total)) return set_err(h, PIC_ERR_ARG, "bad profile");
+    for (int i = 0; i < g.nx; i++)
+        for (int l = 0; l < g.ny; l++)
+            for (int k = 0; k < g.nz; k++) tcount[g.tile_of_cell(i, l, k)] += cnt[g.dense_of(i, l, k)];
+    rc = alloc_species(h, species, tcount);
+    if (rc) return rc;
+    // slots of a tile: its cells in (i, l, k) order, z fastest (the order the bin sort restores)
+    const std::vector<int> &start = h->sp[species].h_start;
+    std::vector<int> fill(g.ntiles, 0);
+    for (int i = 0; i < g.nx; i++)
+        for (int l = 0; l < g.ny; l++)
+            for (int k = 0; k < g.nz; k++) {
+                const int t = g.tile_of_cell(i, l, k), c = g.dense_of(i, l, k);
+                first[c] = start[t] + fill[t];
+                fill[t] += cnt[c];
+            }
+    int *d = nullptr;
+    CK(cudaMalloc(&d, 2 * (size_t)nc * sizeof(int)), "alloc counts");
+    cudaError_t e = cudaMemcpyAsync(d, cnt.data(), (size_t)nc * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d + nc, first.data(), (size_t)nc * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->sp[species].v.tile_count, tcount.data(), g.ntiles * sizeof(int),
+                            cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = init_cells(g, h->mixed, h->sp[species].v, species, d, d + nc, drift_x, drift_y, drift_z, vth, seed,
+                       h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    CK(e, "init species (profile)");
+    h->kin_valid = 0;
+    return ensure_outbox(h);
+}
+
 int pic_init_species_host(int nx, int ny, int nz, double lx, double ly, double lz, int species_index, int ppc,
                           double drift_x, double drift_y, double drift_z, double vth, uint64_t seed, double *x,
                           double *y, double *z, double *px, double *py, double *pz) {

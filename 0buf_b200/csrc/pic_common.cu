@@ -390,6 +390,39 @@ __global__ void k_init_bins(Grid g, int mixed, SpeciesView S, int species_index,
     }
 }
 
+// seeded generator with per-cell counts: one thread per dense cell writes its
+// cell's particles at slots first[c] .. first[c] + count[c] - 1
+__global__ void k_init_cells(Grid g, int mixed, SpeciesView S, int species_index, const int *__restrict__ count,
+                             const int *__restrict__ first, double dx, double dy, double dz, double vth, uint64_t seed) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.ncells()) return;
+    const int k = c % g.nz, l = (c / g.nz) % g.ny, i = c / (g.nz * g.ny);
+    const int n = count[c], s0 = first[c];
+    const int cell = g.cell_of(i, l, k);
+    for (int q = 0; q < n; q++) {
+        const int slot = s0 + q;
+        const double ox = rng_offset(seed, species_index, c, q, 0);
+        const double oy = rng_offset(seed, species_index, c, q, 1);
+        const double oz = rng_offset(seed, species_index, c, q, 2);
+        double p0 = dx, p1 = dy, p2 = dz;
+        if (vth != 0.0) {
+            p0 = dx + vth * rng_normal(seed, species_index, c, q, 0);
+            p1 = dy + vth * rng_normal(seed, species_index, c, q, 1);
+            p2 = dz + vth * rng_normal(seed, species_index, c, q, 2);
+        }
+        S.cell[slot] = cell;
+        if (!mixed) {
+            S.x[slot] = (double)i * g.hx + ox * g.hx;
+            S.y[slot] = (double)l * g.hy + oy * g.hy;
+            S.z[slot] = (double)k * g.hz + oz * g.hz;
+            S.px[slot] = p0; S.py[slot] = p1; S.pz[slot] = p2;
+        } else {
+            S.ox[slot] = (float)ox; S.oy[slot] = (float)oy; S.oz[slot] = (float)oz;
+            S.fx[slot] = (float)p0; S.fy[slot] = (float)p1; S.fz[slot] = (float)p2;
+        }
+    }
+}
+
 __device__ __forceinline__ double block_sum(double v, double *red) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     __syncthreads();
@@ -558,6 +591,14 @@ cudaError_t init_species_bins(const Grid &g, int mixed, SpeciesView sv, int spec
     int64_t total = (int64_t)g.ncells() * ppc;
     if (total <= 0) return cudaSuccess;
     k_init_bins<<<blocks_for(total, 256), 256, 0, s>>>(g, mixed, sv, species_index, ppc, dx, dy, dz, vth, seed);
+    return cudaGetLastError();
+}
+
+cudaError_t init_cells(const Grid &g, int mixed, SpeciesView sv, int species_index, const int *count,
+                       const int *first, double dx, double dy, double dz, double vth, uint64_t seed, cudaStream_t s) {
+    const int n = g.ncells();
+    if (n <= 0) return cudaSuccess;
+    k_init_cells<<<(n + 127) / 128, 128, 0, s>>>(g, mixed, sv, species_index, count, first, dx, dy, dz, vth, seed);
     return cudaGetLastError();
 }
 

@@ -55,6 +55,9 @@ cudaError_t gather_outbox(const StepParams &p, int species, unsigned n_out, unsi
 // seeded generator straight into bins laid out cell-major within each tile
 cudaError_t init_species_bins(const Grid &g, int mixed, SpeciesView sv, int species_index, int ppc, double dx,
                               double dy, double dz, double vth, uint64_t seed, cudaStream_t s);
+// seeded generator with per-cell counts (count, first slot per dense cell)
+cudaError_t init_cells(const Grid &g, int mixed, SpeciesView sv, int species_index, const int *count,
+                       const int *first, double dx, double dy, double dz, double vth, uint64_t seed, cudaStream_t s);
 // FP64 reductions: out[0] sum E^2, out[1] sum H^2 over nodes 1..N, out[2] sum E^2 all nodes (reference)
 cudaError_t field_energy(const Grid &g, int mixed, const void *const E[3], const void *const H[3], double *out3,
                          cudaStream_t s);

@@ -112,6 +112,15 @@ class PicSimulation:
         self._ck(self.lib.pic_init_species_device(self.h, species, ppc, *[float(d) for d in drift], float(vth),
                                                   int(seed)), "pic_init_species_device")
 
+    def init_species_profile(self, species: int, profile: dict, drift=(0.0, 0.0, 0.0), vth: float = 0.0,
+                             seed: int = 0):
+        """Device generator with per-cell counts from a density profile
+        (keys of ``pic_profile``: ppc_mean, cos_amp, bump_peak, bump_sigma,
+        bump_centre, count_seed)."""
+        prof = make_profile(profile)
+        self._ck(self.lib.pic_init_species_profile(self.h, species, C.byref(prof), *[float(d) for d in drift],
+                                                   float(vth), int(seed)), "pic_init_species_profile")
+
     def num_particles(self, species: int = -1) -> int:
         n = self.lib.pic_num_particles(self.h, species)
         if n < 0:
@@ -291,6 +300,31 @@ def _host_ptr(a):
 
 def _length(a) -> int:
     return int(a.size if isinstance(a, np.ndarray) else a.numel())
+
+
+def make_profile(profile: dict):
+    p = _capi.PicProfile()
+    p.ppc_mean = float(profile["ppc_mean"])
+    p.cos_amp = float(profile.get("cos_amp", 0.0))
+    p.bump_peak = float(profile.get("bump_peak", 1.0))
+    p.bump_sigma = float(profile.get("bump_sigma", 0.0))
+    for a, v in enumerate(profile.get("bump_centre", (-1.0, -1.0, -1.0))):
+        p.bump_centre[a] = float(v)
+    p.count_seed = int(profile.get("count_seed", 0))
+    return p
+
+
+def profile_counts(cells, profile: dict) -> np.ndarray:
+    """Particles per cell of a density profile (``pic_profile_counts``), shape cells."""
+    lib = _capi.load()
+    counts = np.zeros(int(np.prod(cells)), np.int32)
+    total = C.c_int64(0)
+    prof = make_profile(profile)
+    rc = lib.pic_profile_counts(int(cells[0]), int(cells[1]), int(cells[2]), C.byref(prof),
+                                counts.ctypes.data_as(_capi.I32), C.byref(total))
+    if rc != 0:
+        raise PicError(rc, "pic_profile_counts")
+    return counts.reshape(tuple(int(c) for c in cells))
 
 
 def host_species(cells, lengths, species_index: int, ppc: int, drift=(0.0, 0.0, 0.0), vth: float = 0.0,

@@ -174,8 +174,7 @@ def make_sim(pkg, cfg, form, device, seed_base):
     cells, h, tau, ppc = cfg["cells"], cfg["h"], cfg["tau"], cfg["ppc"]
     box = tuple(c * h for c in cells)
     sim = pkg.PicSimulation(cells, box, tau, pkg.configs.species_table(ppc), precision=form, device=device)
-    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
-        sim.init_species(i, ppc, s["drift"], s["vth"], seed_base + i)
+    pkg.configs.init_config_species(sim, cfg, seed_base)
     return sim
 
 

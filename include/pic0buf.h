@@ -125,6 +125,30 @@ int pic_get_particles_cells(pic_handle *h, int species, int64_t cap, int32_t *ce
  * drift + vth * N(0,1) per axis.  Keyed by (seed, species, cell, slot). */
 int pic_init_species_device(pic_handle *h, int species, int ppc, double drift_x, double drift_y,
                             double drift_z, double vth, uint64_t seed);
+/* Non-uniform density for the stress configuration (no counterpart in the
+ * reference, whose loader is uniform): the expected count of cell (i,l,k) is
+ *   ppc_mean * f(i,l,k) / mean over cells of f,
+ *   f = (1 + cos_amp cos(2 pi (i + 1/2) / Nx))
+ *       * (1 + (bump_peak - 1) exp(-d^2 / (2 bump_sigma^2))),
+ * d = distance in cells from the cell centre to bump_centre (the box centre
+ * when any of its components is negative), rounded up or down at random
+ * keyed by (count_seed, cell) -- two species with the same profile and
+ * count_seed get the same count in every cell. */
+typedef struct pic_profile {
+    double ppc_mean;
+    double cos_amp;
+    double bump_peak;
+    double bump_sigma;
+    double bump_centre[3];
+    uint64_t count_seed;
+} pic_profile;
+/* Particles per cell of a profile (host, no GPU): counts[dense cell], dense
+ * cell = (i*Ny + l)*Nz + k.  Returns the total in *total. */
+int pic_profile_counts(int nx, int ny, int nz, const pic_profile *prof, int32_t *counts, int64_t *total);
+/* The device generator with per-cell counts from a profile; particles are
+ * keyed by (seed, species, cell, slot) like pic_init_species_device. */
+int pic_init_species_profile(pic_handle *h, int species, const pic_profile *prof, double drift_x, double drift_y,
+                             double drift_z, double vth, uint64_t seed);
 /* The same generator on the host (writes n = Nx*Ny*Nz*ppc particles). */
 int pic_init_species_host(int nx, int ny, int nz, double lx, double ly, double lz, int species_index, int ppc,
                           double drift_x, double drift_y, double drift_z, double vth, uint64_t seed,

@@ -122,3 +122,22 @@ def test_configs(pkg):
     assert t[2][1] == pytest.approx(-0.01 / 32)
     n = np.prod(c.CONFIGS["c2"]["cells"]) * 3 * c.CONFIGS["c2"]["ppc"]
     assert n == 805306368
+
+
+def test_profile_counts(pkg):
+    """The stress configuration's density profile: mean ppc, cos modulation in
+    x, the bump at the box centre, identical counts for the same count seed."""
+    cells = (32, 16, 16)
+    prof = dict(pkg.configs.C4_PROFILE, ppc_mean=20)
+    n = pkg.profile_counts(cells, prof)
+    assert n.shape == cells
+    assert abs(n.mean() - 20) < 0.05
+    assert n[15:17, 7:9, 7:9].max() >= n.max() - 1 and n.max() > 2 * 20
+    assert np.array_equal(n, pkg.profile_counts(cells, prof))
+    other = pkg.profile_counts(cells, dict(prof, count_seed=prof["count_seed"] + 1))
+    assert not np.array_equal(n, other) and abs(other.mean() - 20) < 0.05
+    flat = pkg.profile_counts(cells, dict(ppc_mean=20, cos_amp=0.5, bump_peak=1.0))
+    # 1 + 0.5 cos(2 pi (i + 1/2) / Nx): densest at i = 0, thinnest at i = Nx/2
+    assert flat[0].mean() > 1.4 * 20 and flat[16].mean() < 0.6 * 20
+    with pytest.raises(pkg.PicError):
+        pkg.profile_counts(cells, dict(ppc_mean=20, bump_peak=2.0, bump_sigma=0.0))
