@@ -128,6 +128,7 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
 }
 
 int ensure_outbox(pic_handle *h) {
+    if (h->outbox_pinned) return PIC_OK;  // leftovers of an overflowing insert still live in it
     int64_t total = 0;
     for (int s = 0; s < h->cfg.nspecies; s++) total += h->sp[s].cap_total;
     double frac = h->cfg.outbox_fraction > 0 ? h->cfg.outbox_fraction : 0.04;
@@ -266,10 +267,16 @@ int check_status(pic_handle *h) {
     }
     if (st.flags & ST_TILE_FULL) {
         unsigned n_out = st.out_count < h->out_cap ? st.out_count : h->out_cap;
+        // the outbox keeps every species' leftovers until the last species has
+        // taken its own: a rebin must not resize (and so clear) it on the way
+        h->outbox_pinned = 1;
         for (int s = 0; s < h->cfg.nspecies; s++) {
             int rc = rebin_species(h, s, n_out);
-            if (rc) return rc;
+            if (rc) { h->outbox_pinned = 0; return rc; }
         }
+        h->outbox_pinned = 0;
+        int rc = ensure_outbox(h);
+        if (rc) return rc;
         // leftovers are in the bins now
         CK(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), h->stream), "reset status");
         h->kin_valid = 0;

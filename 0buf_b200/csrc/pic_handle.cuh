@@ -34,6 +34,7 @@ struct pic_handle {
     int64_t sorts;  // tile sorts run by the last step
     void *outbox;
     unsigned out_cap;
+    int outbox_pinned;  // set while a multi-species rebin still reads leftovers from the outbox
     size_t out_elem;
     pic::DevStatus *st;
     pic::DevStatus *st_host;

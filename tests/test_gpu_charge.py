@@ -116,3 +116,23 @@ def test_momentum_matches_particles(pkg, precision):
             M = sim.cfg.species[s].m / sim.cfg.species[s].q_m
             ref = M * np.array([p["px"].sum(), p["py"].sum(), p["pz"].sum()])
             np.testing.assert_allclose(P[s], ref, rtol=1e-12, atol=1e-15 * abs(M) * p["px"].size)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 1e-5)])
+def test_long_run_conserves_particles_and_charge(pkg, precision, tol):
+    """1000 steps of the c2 species on 128x32x32 cells (12.6M particles): the
+    beam bunches, tiles overflow and the step rebins.  Regression: a rebin of
+    one species could resize the outbox while later species' overflow
+    leftovers were still in it, silently losing particles (found by the
+    Gauss-law check).  Every species keeps its particles and G stays put."""
+    cells, ppc = (128, 32, 32), 32
+    cfg = dict(pkg.configs.CONFIGS["c2"], cells=cells, ppc=ppc)
+    with pkg.PicSimulation(cells, tuple(c * cfg["h"] for c in cells), cfg["tau"], pkg.configs.species_table(ppc),
+                           precision=precision) as sim:
+        pkg.configs.init_config_species(sim, cfg, 0)
+        n0 = [sim.num_particles(s) for s in range(3)]
+        sim.gauss_check(set_baseline=True)
+        sim.run(1000)
+        assert [sim.num_particles(s) for s in range(3)] == n0
+        g = sim.gauss_check()
+        assert g[0] < tol * g[1], g
