@@ -174,6 +174,8 @@ __device__ __forceinline__ PartM load_part(const SpeciesView &S, int slot) {
 constexpr int kGroups = 4;
 constexpr int kSlots = 54;
 constexpr int kQueue = 64;  // queued segments per warp
+static_assert(kHoleMax * sizeof(int) <= (kPushThreads / 32) * kQueue * 2 * sizeof(float4),
+              "the compaction's front-hole list lives in the queues' memory");
 
 // w (in units of 2^e_w) -> units of 2^e_tile, sh = e_w - e_tile, round half up
 __device__ __forceinline__ long long rescale(int w, int sh) {
@@ -187,7 +189,9 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     __shared__ double sQ;
     __shared__ int sTileE;
     __shared__ float sInvQ;
-    __shared__ int sWarpAcc[kPushThreads / 32][kGroups * kSlots];
+    // two per-warp group buffers: the flush of one iteration's sums runs in the
+    // next iteration, after their shared-memory atomics have completed
+    __shared__ int sWarpAcc[kPushThreads / 32][2][kGroups * kSlots];
     __shared__ int sSlotNode[kSlots];
     // queued segments: {stencil origin node, class bits, start x,y,z, end x,y,z}
     __shared__ float4 sQueue[kPushThreads / 32][kQueue][2];
@@ -203,8 +207,9 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
     float4 *sF = (float4 *)smem_raw;  // Ex Ey Ez Hx Hy Hz
     unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);
     int *sHoles = (int *)(sJ + 3 * nn);
-    int *sFront = sHoles + kHoleMax;
-    int *wacc = sWarpAcc[warp];
+    // the front-hole list of the compaction reuses the (then drained) queues
+    int *sFront = (int *)&sQueue[0][0][0];
+    int *wacc = &sWarpAcc[warp][0][0];
     if (threadIdx.x == 0) {
         // quantum of the fixed-point tile J (see fx_add): |contribution| < 1.0834 |m| per segment
         double bound = 0.0;
@@ -215,7 +220,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
         sTileE = e2 - 62;  // tile quantum 2^(e2-62)
         sInvQ = (float)ldexp(1.0, 62 - e2);
     }
-    for (int e = lane; e < kGroups * kSlots; e += 32) wacc[e] = 0;
+    for (int e = lane; e < 2 * kGroups * kSlots; e += 32) wacc[e] = 0;
     if (threadIdx.x < kSlots) {
         // slot -> tile-local node offset from a cell's stencil origin (local index 0,0,0)
         const int e = threadIdx.x;
@@ -289,6 +294,35 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
         };
         auto drain = [&](int n) { drain_range(0, n); };
         auto drain_top32 = [&](int n) { drain_range(n - 32, 32); };
+        // add the group sums of buffer buf (groups led by the lanes of lead, stencil
+        // origins n0v, warp/tile quantum shift shv) into the tile J and clear them;
+        // exact: both quanta are powers of two, the tile bound keeps the sum below 2^62
+        auto flush_groups = [&](int *buf, unsigned lead, int n0v, int shv) {
+            unsigned lm = lead;
+            for (int gi = 0; gi < kGroups && lm; gi++) {
+                const int ld = __ffs(lm) - 1;
+                lm &= lm - 1;
+                const int base = __shfl_sync(FULL, n0v, ld);
+                int *wg = buf + gi * kSlots;
+                int w = wg[lane];
+                if (w) {
+                    wg[lane] = 0;
+                    const long long add = rescale(w, shv);
+                    if (add) atomicAdd(&sJ[base + slotA], (unsigned long long)add);
+                }
+                if (lane < kSlots - 32) {
+                    w = wg[32 + lane];
+                    if (w) {
+                        wg[32 + lane] = 0;
+                        const long long add = rescale(w, shv);
+                        if (add) atomicAdd(&sJ[base + slotB], (unsigned long long)add);
+                    }
+                }
+            }
+        };
+        int gbuf = 0;  // buffer of this iteration's sums; the other one holds the pending ones
+        unsigned pend_lead = 0;
+        int pend_n0 = 0, pend_sh = 0;
         // warp-synchronous loop: every lane of a warp runs the same iterations;
         // the next particle is loaded before the current one is processed
         const int stride = blockDim.x;
@@ -392,10 +426,11 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
             const bool cross = dep && (i2[0] != i1x || i2[1] != i1y || i2[2] != i1z);
             float x2[3] = {xe[0], xe[1], xe[2]};
             if (cross) split_point(i1, i2, xs, xe, x2);
+            flush_groups(wacc + (gbuf ^ 1) * (kGroups * kSlots), pend_lead, pend_n0, pend_sh);
             if (fast) {
                 float v[12];
                 pqr_mixed(i1, xs, x2, wx, wy, wz, v);
-                int *wb = wacc + grp * kSlots;
+                int *wb = wacc + gbuf * (kGroups * kSlots) + grp * kSlots;
                 const int cx = i1x - 2, cy = i1y - 2, cz = i1z - 2;
                 const int bx = cx * 9 + cy * 3 + cz, by = 18 + cx * 6 + cy * 3 + cz, bz = 36 + cx * 6 + cy * 2 + cz;
                 const int off[12] = {bx, bx + 1, bx + 3, bx + 4, by, by + 1, by + 6, by + 7, bz, bz + 2, bz + 6, bz + 8};
@@ -437,32 +472,10 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
                     }
                 }
             }
-            __syncwarp();
-            // flush the per-warp group sums into the tile J (exact: both quanta are
-            // powers of two, the tile bound keeps the result below 2^62)
-            {
-                unsigned lm = leaders;
-                for (int gi = 0; gi < kGroups && lm; gi++) {
-                    const int ld = __ffs(lm) - 1;
-                    lm &= lm - 1;
-                    const int base = __shfl_sync(FULL, n0, ld);
-                    int *wg = wacc + gi * kSlots;
-                    int w = wg[lane];
-                    if (w) {
-                        wg[lane] = 0;
-                        const long long add = rescale(w, sh);
-                        if (add) atomicAdd(&sJ[base + slotA], (unsigned long long)add);
-                    }
-                    if (lane < kSlots - 32) {
-                        w = wg[32 + lane];
-                        if (w) {
-                            wg[32 + lane] = 0;
-                            const long long add = rescale(w, sh);
-                            if (add) atomicAdd(&sJ[base + slotB], (unsigned long long)add);
-                        }
-                    }
-                }
-            }
+            pend_lead = leaders;
+            pend_n0 = n0;
+            pend_sh = sh;
+            gbuf ^= 1;
             __syncwarp();
 
             if (!active) continue;
@@ -504,6 +517,8 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
                 else bad |= ST_HOLES;
             }
         }
+        flush_groups(wacc + (gbuf ^ 1) * (kGroups * kSlots), pend_lead, pend_n0, pend_sh);
+        __syncwarp();
         drain(qn);
         if (unsorted) atomicAdd(&P.st->unsorted[s], (unsigned long long)unsorted);
         __syncthreads();
@@ -571,7 +586,7 @@ void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], dou
 
 size_t push_smem_mixed(const Grid &g) {
     size_t nn = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2);
-    return 6 * nn * sizeof(float4) + 3 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
+    return 6 * nn * sizeof(float4) + 3 * nn * sizeof(unsigned long long) + kHoleMax * sizeof(int);
 }
 
 size_t push_smem_total_mixed(const Grid &g) {
