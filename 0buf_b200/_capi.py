@@ -113,6 +113,7 @@ SIGNATURES = {
     "pic_layout_info": (C.c_int, [H, I64]),
     "pic_stream": (C.c_void_p, [H]),
     "pic_forward": (C.c_int, [H, C.c_int, C.c_int]),
+    "pic_forward2": (C.c_int, [H, C.c_int, C.c_int, C.c_int]),
     "pic_forward_history": (C.c_int, [H, D]),
     "pic_loss_value": (C.c_int, [H, C.POINTER(PicLoss), D]),
     "pic_backward": (C.c_int, [H, C.POINTER(PicLoss), C.POINTER(PicGrads)]),

@@ -1031,8 +1031,8 @@ namespace pic_host {
 void adj_free(pic_handle *h) {
     if (!h || !h->adj) return;
     AdjState *A = h->adj;
-    void *bufs[] = {A->cur, A->ckp, A->ckf, A->segp, A->segf, A->lamp, A->lamf, A->rf, A->ha, A->hist, A->st,
-                    A->red, A->lamF, A->segF};
+    void *bufs[] = {A->cur, A->ckp, A->ckf, A->segp, A->segf, A->subp, A->subf, A->lamp, A->lamf, A->rf, A->ha,
+                    A->hist, A->st, A->red, A->lamF, A->segF};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (A->e0) cudaEventDestroy(A->e0);
@@ -1251,25 +1251,48 @@ int backward_run(pic_handle *h, AdjState &A, const pic_loss &L) {
     void *RF[PIC_FIELD_COUNT];
     rf_view(h, A, RF);
     CK(cudaEventRecord(A.e0, st), "event");
+    const size_t ehb = 6 * fbytes;  // E and H of one state (the first arrays of rf)
     for (int seg = A.nseg - 1; seg >= 0; seg--) {
-        int start = seg * A.K, end = std::min(start + A.K, A.steps), len = end - start;
-        CK(cudaMemcpyAsync(A.segp, A.ckp + (size_t)seg * A.pbytes, A.pbytes, cudaMemcpyDeviceToDevice, st), "restore");
-        CK(cudaMemcpyAsync(A.rf, A.ckf + (size_t)seg * 6 * fbytes, 6 * fbytes, cudaMemcpyDeviceToDevice, st),
-           "restore fields");
-        for (int j = 0; j < len; j++) {
-            CK(cudaMemcpyAsync(A.segf + (size_t)j * 6 * fbytes, A.rf, 6 * fbytes, cudaMemcpyDeviceToDevice, st),
-               "keep fields");
-            void *Fj = A.segF ? (char *)A.segF + (size_t)j * Fstep : nullptr;
-            int rc = flat_step(h, A, A.segp + (size_t)j * A.pbytes, RF, A.segp + (size_t)(j + 1) * A.pbytes, Fj);
-            if (rc) return rc;
+        const int start = seg * A.K, end = std::min(start + A.K, A.steps), len = end - start;
+        const int K2 = A.K2, nsub = (len + K2 - 1) / K2;
+        if (nsub > 1) {
+            // second level: recompute the segment once, keeping the state and E/H at
+            // the start of every sub-segment (the running state lives in segp[0])
+            CK(cudaMemcpyAsync(A.segp, A.ckp + (size_t)seg * A.pbytes, A.pbytes, cudaMemcpyDeviceToDevice, st),
+               "restore");
+            CK(cudaMemcpyAsync(A.rf, A.ckf + (size_t)seg * ehb, ehb, cudaMemcpyDeviceToDevice, st), "restore fields");
+            for (int j = 0; j < len; j++) {
+                if (j % K2 == 0) {
+                    const int q = j / K2;
+                    CK(cudaMemcpyAsync(A.subp + (size_t)q * A.pbytes, A.segp, A.pbytes, cudaMemcpyDeviceToDevice, st),
+                       "sub-checkpoint");
+                    CK(cudaMemcpyAsync(A.subf + (size_t)q * ehb, A.rf, ehb, cudaMemcpyDeviceToDevice, st),
+                       "sub-checkpoint fields");
+                    if (q == nsub - 1) break;  // the last sub-segment starts here
+                }
+                int rc = flat_step(h, A, A.segp, RF, nullptr, nullptr);
+                if (rc) return rc;
+            }
         }
-        CK(cudaMemcpyAsync(A.segf + (size_t)len * 6 * fbytes, A.rf, 6 * fbytes, cudaMemcpyDeviceToDevice, st),
-           "keep fields");
-        for (int j = len - 1; j >= 0; j--) {
-            int rc = reverse_step(h, A, L, start + j, A.segp + (size_t)j * A.pbytes, A.segf + (size_t)j * 6 * fbytes,
-                                  A.segf + (size_t)(j + 1) * 6 * fbytes,
-                                  A.segF ? (const char *)A.segF + (size_t)j * Fstep : nullptr);
-            if (rc) return rc;
+        for (int q = nsub - 1; q >= 0; q--) {
+            const int s0 = start + q * K2, s1 = std::min(s0 + K2, end), slen = s1 - s0;
+            const char *sp = nsub > 1 ? A.subp + (size_t)q * A.pbytes : A.ckp + (size_t)seg * A.pbytes;
+            const char *sf = nsub > 1 ? A.subf + (size_t)q * ehb : A.ckf + (size_t)seg * ehb;
+            CK(cudaMemcpyAsync(A.segp, sp, A.pbytes, cudaMemcpyDeviceToDevice, st), "restore");
+            CK(cudaMemcpyAsync(A.rf, sf, ehb, cudaMemcpyDeviceToDevice, st), "restore fields");
+            for (int j = 0; j < slen; j++) {
+                CK(cudaMemcpyAsync(A.segf + (size_t)j * ehb, A.rf, ehb, cudaMemcpyDeviceToDevice, st), "keep fields");
+                void *Fj = A.segF ? (char *)A.segF + (size_t)j * Fstep : nullptr;
+                int rc = flat_step(h, A, A.segp + (size_t)j * A.pbytes, RF, A.segp + (size_t)(j + 1) * A.pbytes, Fj);
+                if (rc) return rc;
+            }
+            CK(cudaMemcpyAsync(A.segf + (size_t)slen * ehb, A.rf, ehb, cudaMemcpyDeviceToDevice, st), "keep fields");
+            for (int j = slen - 1; j >= 0; j--) {
+                int rc = reverse_step(h, A, L, s0 + j, A.segp + (size_t)j * A.pbytes, A.segf + (size_t)j * ehb,
+                                      A.segf + (size_t)(j + 1) * ehb,
+                                      A.segF ? (const char *)A.segF + (size_t)j * Fstep : nullptr);
+                if (rc) return rc;
+            }
         }
     }
     CK(cudaEventRecord(A.e1, st), "event");
@@ -1281,9 +1304,13 @@ int backward_run(pic_handle *h, AdjState &A, const pic_loss &L) {
 // ============================================================ C ABI ==
 extern "C" {
 
-int pic_forward(pic_handle *h, int steps, int ckpt_every) {
+int pic_forward(pic_handle *h, int steps, int ckpt_every) { return pic_forward2(h, steps, ckpt_every, ckpt_every); }
+
+int pic_forward2(pic_handle *h, int steps, int ckpt_every, int sub_every) {
     if (!h) return PIC_ERR_ARG;
     if (steps < 1 || ckpt_every < 1) return set_err(h, PIC_ERR_ARG, "pic_forward: steps and ckpt_every must be >= 1");
+    if (sub_every < 1 || sub_every > ckpt_every)
+        return set_err(h, PIC_ERR_ARG, "pic_forward2: sub_every must be in 1..ckpt_every");
     int rc = set_device(h);
     if (rc) return rc;
     if ((rc = need_particles(h))) return rc;
@@ -1296,6 +1323,7 @@ int pic_forward(pic_handle *h, int steps, int ckpt_every) {
     A.nsp = h->cfg.nspecies;
     A.steps = steps;
     A.K = ckpt_every;
+    A.K2 = sub_every;
     A.nseg = (steps + ckpt_every - 1) / ckpt_every;
     const Grid &g = h->g;
     std::vector<std::vector<int>> counts(A.nsp);
@@ -1398,8 +1426,13 @@ int pic_backward(pic_handle *h, const pic_loss *loss, pic_grads *grads) {
     const size_t fbytes = N * (h->mixed ? sizeof(float) : sizeof(double));
     int64_t np = total_particles(A);
     if (!A.segp) {
-        if ((rc = adj_alloc(h, (void **)&A.segp, A.pbytes * (size_t)(A.K + 1), "the segment states"))) return rc;
-        if ((rc = adj_alloc(h, (void **)&A.segf, fbytes * 6 * (size_t)(A.K + 1), "the segment fields"))) return rc;
+        if ((rc = adj_alloc(h, (void **)&A.segp, A.pbytes * (size_t)(A.K2 + 1), "the segment states"))) return rc;
+        if ((rc = adj_alloc(h, (void **)&A.segf, fbytes * 6 * (size_t)(A.K2 + 1), "the segment fields"))) return rc;
+        if (A.K2 < A.K) {
+            const size_t nsub = (size_t)(A.K + A.K2 - 1) / A.K2;
+            if ((rc = adj_alloc(h, (void **)&A.subp, A.pbytes * nsub, "the sub-checkpoint states"))) return rc;
+            if ((rc = adj_alloc(h, (void **)&A.subf, fbytes * 6 * nsub, "the sub-checkpoint fields"))) return rc;
+        }
         A.lamp_bytes = (size_t)np * 6 * A.elem;
         if ((rc = adj_alloc(h, (void **)&A.lamp, A.lamp_bytes, "the particle adjoints"))) return rc;
         if ((rc = adj_alloc(h, (void **)&A.lamf, N * sizeof(double) * 12, "the field adjoints"))) return rc;
@@ -1411,7 +1444,7 @@ int pic_backward(pic_handle *h, const pic_loss *loss, pic_grads *grads) {
         // adjoint does not gather them again (skipped when memory is short)
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        size_t want = (size_t)np * 6 * A.elem * (size_t)A.K;
+        size_t want = (size_t)np * 6 * A.elem * (size_t)A.K2;
         if (want + ((size_t)4 << 30) < free_b && cudaMalloc((void **)&A.segF, want) != cudaSuccess) {
             A.segF = nullptr;
             cudaGetLastError();

@@ -28,12 +28,15 @@ struct AdjState {
     int nsp;
     int64_t n[kMaxSpecies];
     int steps, K, nseg;
+    int K2;            // sub-checkpoint interval inside a segment (== K: one level)
     size_t pbytes;     // one particle state
     char *cur;         // the forward's running state
     char *ckp;         // nseg particle checkpoints
     char *ckf;         // nseg x (E, H): 6 field arrays each, in the form's field type
-    char *segp;        // K+1 particle states of the segment being reversed
-    char *segf;        // K+1 x (E, H) of that segment
+    char *segp;        // K2+1 particle states of the (sub-)segment being reversed
+    char *segf;        // K2+1 x (E, H) of that (sub-)segment
+    char *subp;        // two levels: ceil(K/K2) sub-checkpoint states of the segment being reversed
+    char *subf;        // two levels: their (E, H)
     char *lamp;        // per species lambda_x (3) and lambda_p (3), form's element type
     size_t lamp_bytes;
     double *lamf;      // FP64 lambda_E, lambda_H, lambda_J, lambda_Q (12 arrays)

@@ -235,9 +235,13 @@ class PicSimulation:
         return dict(tiles=int(v[0]), slots=int(v[1]), bytes_per_particle=int(v[2]), nodes=int(v[3]))
 
     # ------------------------------------------------- differentiable run
-    def forward(self, steps: int, ckpt_every: int):
-        """``pic_forward``: advance ``steps`` steps, checkpointing every ``ckpt_every``."""
-        self._ck(self.lib.pic_forward(self.h, int(steps), int(ckpt_every)), "pic_forward")
+    def forward(self, steps: int, ckpt_every: int, sub_every: int | None = None):
+        """``pic_forward``: advance ``steps`` steps, checkpointing every ``ckpt_every``
+        (``pic_forward2`` with a second checkpoint level every ``sub_every`` steps)."""
+        if sub_every is None:
+            self._ck(self.lib.pic_forward(self.h, int(steps), int(ckpt_every)), "pic_forward")
+        else:
+            self._ck(self.lib.pic_forward2(self.h, int(steps), int(ckpt_every), int(sub_every)), "pic_forward2")
         self._fwd_steps = int(steps)
 
     def history(self) -> np.ndarray:

@@ -302,6 +302,8 @@ def run_ours(args, dist):
         out["e2e"] = run_e2e(args, dist, pkg, cfg, form, torch, n_local)
     if dist.world == 1 and not args.no_adjoint:
         out["adjoint"] = run_adjoint(args, pkg, dev)
+    if dist.world == 1 and args.stress_adjoint:
+        out["adjoint_stress"] = run_adjoint_stress(args, pkg, dev)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
@@ -439,6 +441,47 @@ def run_adjoint(args, pkg, dev):
             fd[form][k] = [float(f"{x:.3e}") for x in v] if isinstance(v, list) else float(f"{v:.3e}")
     out["fd_check"] = {"reference": "FP64 central differences of the FP64 forward", "fd_drift": d_drift,
                        "fd_vth": d_vth, **fd}
+    return out
+
+
+def run_adjoint_stress(args, pkg, dev):
+    """The stress configuration's differentiable run at full size: FP32
+    forward of 500 steps with two checkpoint levels (segments of 63 steps,
+    a sub-checkpoint every 8) and the backward of the adjoint configuration's
+    loss, checked against FP64 central differences along the beam drift
+    (eps 1e-8, two FP64 forwards without checkpoints)."""
+    import numpy as np
+    cfg = dict(pkg.configs.CONFIGS["c4"])
+    steps, K, K2 = cfg["steps"], 63, 8
+    sim = make_sim(pkg, cfg, "fp32", dev, 0)
+    n = sim.num_particles()
+    sim.forward(steps, K, K2)
+    g = sim.backward(want_p0=False, **ADJ_LOSS)
+    t = sim.adjoint_timings()
+    sim.close()
+    out = {"config": f"c4: {'x'.join(map(str, cfg['cells']))} cells, {n:,} particles, {steps} steps, FP32, "
+                     f"checkpoints every {K} steps with sub-checkpoints every {K2}, loss of the adjoint configuration",
+           "forward_ms": round(float(t[0]), 1), "backward_ms": round(float(t[1]), 1),
+           "backward_over_forward": round(float(t[1] / t[0]), 3),
+           "loss": g["loss"], "d_drift_x": float(g["d_drift"][0]), "d_vth": float(g["d_vth"])}
+    if not args.no_fd:
+        keys = ("x", "y", "z", "px", "py", "pz")
+        ref = make_sim(pkg, cfg, "fp64", dev, 0)
+        base = ref.particles(ADJ_LOSS["species"])
+        ref.close()
+        vals = []
+        eps = 1e-8
+        for sg in (1.0, -1.0):
+            s = make_sim(pkg, cfg, "fp64", dev, 0)
+            b = {k: base[k] for k in keys}
+            b["px"] = base["px"] + sg * eps
+            s.load_particles(ADJ_LOSS["species"], *[b[k] for k in keys])
+            s.forward(steps, steps)
+            vals.append(s.loss_value(field="Ex", window=ADJ_LOSS["window"]))
+            s.close()
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        out["fd_drift_fp64"] = fd
+        out["drift_rel_err"] = float(f"{abs(g['d_drift'][0] - fd) / abs(fd):.3e}")
     return out
 
 
@@ -600,6 +643,9 @@ def main():
     ap.add_argument("--adjoint-dirs", type=int, default=4,
                     help="random single-particle directions of the finite-difference check")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--stress-adjoint", action="store_true",
+                    help="also run the stress configuration's differentiable run at full size (FP32, two checkpoint levels)")
+    ap.add_argument("--no-fd", action="store_true", help="skip the finite-difference reference of --stress-adjoint")
     ap.add_argument("--accuracy-steps", type=int, default=0,
                     help="also run both forms this many steps with energies every step (FP32 error history)")
     ap.add_argument("--reference-inner", type=int, default=20)

@@ -261,6 +261,13 @@ typedef struct pic_grads {
 } pic_grads;
 
 int pic_forward(pic_handle *h, int steps, int ckpt_every);
+/* pic_forward with two checkpoint levels for runs whose states do not fit:
+ * pic_backward recomputes each ckpt_every-step segment once to keep a state
+ * every sub_every steps, then each sub-segment again to reverse it.  Device
+ * memory: about steps/ckpt_every + ckpt_every/sub_every + sub_every + 1
+ * particle states instead of steps/ckpt_every + ckpt_every + 1, for one more
+ * forward recomputation.  sub_every = ckpt_every is pic_forward. */
+int pic_forward2(pic_handle *h, int steps, int ckpt_every, int sub_every);
 /* out[n*3 + c] = W[n][c] of the last forward run (host array of 3*steps) */
 int pic_forward_history(pic_handle *h, double *out);
 int pic_loss_value(pic_handle *h, const pic_loss *loss, double *value);

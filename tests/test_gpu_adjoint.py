@@ -112,15 +112,21 @@ def test_gradient_matches_finite_differences(pkg):
     assert max(errs.values()) < 1e-3, errs
 
 
-def test_gradient_independent_of_checkpoints(pkg):
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gradient_independent_of_checkpoints(pkg, precision):
+    """One level (K = 1, 7, 30) and two levels (pic_forward2: segments of 12
+    or 30 steps with a sub-checkpoint every 4 or 7) give the same gradient."""
     grads = []
-    for K in (1, 7, STEPS):
-        with make(pkg) as sim:
-            sim.forward(STEPS, K)
+    for K, K2 in ((1, None), (7, None), (STEPS, None), (12, 4), (STEPS, 7)):
+        with make(pkg, precision=precision) as sim:
+            sim.forward(STEPS, K, K2)
             grads.append(sim.backward(**LOSS))
+    # FP64 recomputes are reproducible to rounding; the FP32 form's recomputed
+    # steps add the FP64 current in no fixed order, which can move an FP32 ulp
+    tol = 1e-9 if precision == "fp64" else 1e-4
     for g in grads[1:]:
-        assert rel_l2(g["d_p0"], grads[0]["d_p0"]) < 1e-9
-        np.testing.assert_allclose(g["d_drift"], grads[0]["d_drift"], rtol=1e-9)
+        assert rel_l2(g["d_p0"], grads[0]["d_p0"]) < tol
+        np.testing.assert_allclose(g["d_drift"], grads[0]["d_drift"], rtol=tol)
 
 
 def test_mixed_forward_is_the_step(pkg):
