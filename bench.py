@@ -448,8 +448,18 @@ def run_adjoint_stress(args, pkg, dev):
     """The stress configuration's differentiable run at full size: FP32
     forward of 500 steps with two checkpoint levels (segments of 63 steps,
     a sub-checkpoint every 8) and the backward of the adjoint configuration's
-    loss, checked against FP64 central differences along the beam drift
-    (eps 1e-8, two FP64 forwards without checkpoints)."""
+    loss, checked against FP64 differences along the beam drift.
+
+    The reference differences need a very small eps.  The hot electrons
+    cross cell-centre planes all the time, and the zigzag deposit is
+    continuous but not differentiable where a step starts or stops crossing
+    one (kinks); its relay point even jumps where a step switches between
+    crossing one plane and two.  Over 500 steps the perturbation grows, and
+    with eps >= 1e-12 the +-eps interval holds such events (measured:
+    central differences of 0.97, 0.58 and 0.24 at eps 1e-10, 1e-11 and
+    1e-12, against about 0.45).  eps = 1e-13 is used: the central difference
+    and both one-sided differences are reported, with the noise floor from
+    two identical FP64 runs (the FP64 current is added in no fixed order)."""
     import numpy as np
     cfg = dict(pkg.configs.CONFIGS["c4"])
     steps, K, K2 = cfg["steps"], 63, 8
@@ -469,19 +479,25 @@ def run_adjoint_stress(args, pkg, dev):
         ref = make_sim(pkg, cfg, "fp64", dev, 0)
         base = ref.particles(ADJ_LOSS["species"])
         ref.close()
-        vals = []
-        eps = 1e-8
-        for sg in (1.0, -1.0):
+
+        def loss_at(d):
             s = make_sim(pkg, cfg, "fp64", dev, 0)
             b = {k: base[k] for k in keys}
-            b["px"] = base["px"] + sg * eps
+            b["px"] = base["px"] + d
             s.load_particles(ADJ_LOSS["species"], *[b[k] for k in keys])
             s.forward(steps, steps)
-            vals.append(s.loss_value(field="Ex", window=ADJ_LOSS["window"]))
+            v = s.loss_value(field="Ex", window=ADJ_LOSS["window"])
             s.close()
-        fd = (vals[0] - vals[1]) / (2 * eps)
-        out["fd_drift_fp64"] = fd
-        out["drift_rel_err"] = float(f"{abs(g['d_drift'][0] - fd) / abs(fd):.3e}")
+            return v
+
+        eps = 1e-13
+        l0, l0b, lp, lm = loss_at(0.0), loss_at(0.0), loss_at(eps), loss_at(-eps)
+        central = (lp - lm) / (2 * eps)
+        ad = float(g["d_drift"][0])
+        out["fd_check"] = {"reference": "FP64 differences of the FP64 forward along the beam drift, eps 1e-13",
+                           "central": central, "forward": (lp - l0) / eps, "backward": (l0 - lm) / eps,
+                           "noise_floor": abs(l0b - l0) / (2 * eps),
+                           "central_rel_err": float(f"{abs(ad - central) / abs(central):.3e}")}
     return out
 
 
