@@ -114,6 +114,9 @@ SIGNATURES = {
     "pic_stream": (C.c_void_p, [H]),
     "pic_forward": (C.c_int, [H, C.c_int, C.c_int]),
     "pic_forward2": (C.c_int, [H, C.c_int, C.c_int, C.c_int]),
+    "pic_branch_record": (C.c_int, [H, C.c_int]),
+    "pic_forward_replay": (C.c_int, [H, C.c_int, H]),
+    "pic_perturb_momenta": (C.c_int, [H, C.c_int, C.c_int64, D, C.c_double]),
     "pic_forward_history": (C.c_int, [H, D]),
     "pic_loss_value": (C.c_int, [H, C.POINTER(PicLoss), D]),
     "pic_backward": (C.c_int, [H, C.POINTER(PicLoss), C.POINTER(PicGrads)]),

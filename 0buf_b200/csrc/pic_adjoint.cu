@@ -58,6 +58,10 @@ struct FlatParams {
     const double *H[3];
     double *J[3];
     AdjStatus *st;
+    // discrete choices of this step, one 48-bit code per particle (flat index):
+    // bmode 1 records them, 2 replays them (see branch_code)
+    unsigned long long *branch;
+    int bmode;
 };
 // adjoint of one species: lambda_x (3) and lambda_p (3), same order
 struct LamSp {
@@ -96,17 +100,37 @@ struct Taps {
     int tn[3], tc[3];
     double wn[3], wc[3];
 };
-__device__ __forceinline__ void taps_plain(const Grid &g, int i, int l, int k, const double x[3], Taps &T) {
+// the discrete part of the taps: tap indices and the integer parts of the
+// weights (nI = int(x/h + 1), cI = int(x/h + 1.5)); the weights follow from them
+struct TapInts {
+    int tn[3], tc[3], nI[3], cI[3];
+};
+__device__ __forceinline__ void tap_ints(const Grid &g, int i, int l, int k, const double x[3], TapInts &I) {
     const double h3[3] = {g.hx, g.hy, g.hz};
     const int c3[3] = {i, l, k};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         double x0 = (double)c3[d] * h3[d];
-        T.tn[d] = (int)((x[d] - x0) / h3[d] + 1.0) + 1;
-        T.tc[d] = (int)(((x[d] - x0) / h3[d] + 1.0) + 1.5);
-        T.wn[d] = (int)(x[d] / h3[d] + 1.0) - x[d] / h3[d];
-        T.wc[d] = (int)(x[d] / h3[d] + 1.5) - 0.5 - x[d] / h3[d];
+        I.tn[d] = (int)((x[d] - x0) / h3[d] + 1.0) + 1;
+        I.tc[d] = (int)(((x[d] - x0) / h3[d] + 1.0) + 1.5);
+        I.nI[d] = (int)(x[d] / h3[d] + 1.0);
+        I.cI[d] = (int)(x[d] / h3[d] + 1.5);
     }
+}
+__device__ __forceinline__ void taps_from(const Grid &g, const double x[3], const TapInts &I, Taps &T) {
+    const double h3[3] = {g.hx, g.hy, g.hz};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        T.tn[d] = I.tn[d];
+        T.tc[d] = I.tc[d];
+        T.wn[d] = I.nI[d] - x[d] / h3[d];
+        T.wc[d] = I.cI[d] - 0.5 - x[d] / h3[d];
+    }
+}
+__device__ __forceinline__ void taps_plain(const Grid &g, int i, int l, int k, const double x[3], Taps &T) {
+    TapInts I;
+    tap_ints(g, i, l, k, x, I);
+    taps_from(g, x, I, T);
 }
 // component c (0..2 E, 3..5 H) is node-staggered along axis d when
 // (E_c and d == c) or (H_c and d != c)
@@ -140,14 +164,16 @@ __device__ __forceinline__ double interp_g(const double *__restrict__ A, size_t 
 }
 
 // fields at the particle (all six components); false if a stencil left range
-__device__ __forceinline__ bool gather_fields(const Grid &g, const double *const E[3], const double *const H[3],
-                                              int i, int l, int k, const double x[3], double F[6]) {
-    if (x[0] < 0 || x[1] < 0 || x[2] < 0) {
+// (negative_is_zero: the reference's GetField gives no field at a negative
+// coordinate; positions are wrapped into [0, L) so a run never meets it, and a
+// replay of frozen branches, whose wraps are fixed, leaves it out)
+__device__ __forceinline__ bool gather_fields_taps(const Grid &g, const double *const E[3],
+                                                   const double *const H[3], int i, int l, int k, const double x[3],
+                                                   const Taps &T, double F[6], bool negative_is_zero = true) {
+    if (negative_is_zero && (x[0] < 0 || x[1] < 0 || x[2] < 0)) {
         for (int c = 0; c < 6; c++) F[c] = 0.0;
         return true;
     }
-    Taps T;
-    taps_plain(g, i, l, k, x, T);
     const size_t dx = (size_t)g.NY * g.pz, dy = g.pz;
     bool ok = true;
 #pragma unroll
@@ -158,6 +184,12 @@ __device__ __forceinline__ bool gather_fields(const Grid &g, const double *const
         F[c] = interp_g(c < 3 ? E[c] : H[c - 3], tap_node(g, i, l, k, t), dx, dy, w);
     }
     return ok;
+}
+__device__ __forceinline__ bool gather_fields(const Grid &g, const double *const E[3], const double *const H[3],
+                                              int i, int l, int k, const double x[3], double F[6]) {
+    Taps T;
+    taps_plain(g, i, l, k, x, T);
+    return gather_fields_taps(g, E, H, i, l, k, x, T, F);
 }
 
 // Particle::Move, particle.h:65-202, with the intermediates the adjoint needs
@@ -204,20 +236,27 @@ struct Split {
     int m, i1[3], i2[3];
     double x2[3], sr;
 };
-__device__ __forceinline__ void split_plain(const Grid &g, const double xo[3], const double xn[3], const double o3[3],
-                                            Split &S) {
+// the discrete part: cell-centre indices of both end points
+// (getCellNumberCenterCurrent, cell.h:577-578)
+__device__ __forceinline__ void split_ints(const Grid &g, const double xo[3], const double xn[3], const double o3[3],
+                                           Split &S) {
     const double h3[3] = {g.hx, g.hy, g.hz};
-    double *x2 = S.x2;
-    x2[0] = x2[1] = x2[2] = 0.0;
-    S.sr = 0.0;
-    double sr = 0.0;
 #pragma unroll
-    for (int d = 0; d < 3; d++) {  // getCellNumberCenterCurrent, cell.h:577-578
+    for (int d = 0; d < 3; d++) {
         double tt = ((xo[d] - o3[d]) / h3[d] + 1.5);
         S.i1[d] = (int)(tt + 1);
         double t2 = ((xn[d] - o3[d]) / h3[d] + 1.5);
         S.i2[d] = (int)(t2 + 1);
     }
+}
+// the split case and relay point from S.i1, S.i2
+__device__ __forceinline__ void split_from(const Grid &g, const double xo[3], const double xn[3], const double o3[3],
+                                           Split &S) {
+    const double h3[3] = {g.hx, g.hy, g.hz};
+    double *x2 = S.x2;
+    x2[0] = x2[1] = x2[2] = 0.0;
+    S.sr = 0.0;
+    double sr = 0.0;
     const int *i1 = S.i1, *i2 = S.i2;
     int m = 4 * abs(i2[0] - i1[0]) + 2 * abs(i2[1] - i1[1]) + abs(i2[2] - i1[2]);
     S.m = m;
@@ -254,6 +293,11 @@ __device__ __forceinline__ void split_plain(const Grid &g, const double xo[3], c
 #undef RBX
 #undef SQ
     S.sr = sr;
+}
+__device__ __forceinline__ void split_plain(const Grid &g, const double xo[3], const double xn[3], const double o3[3],
+                                            Split &S) {
+    split_ints(g, xo, xn, o3, S);
+    split_from(g, xo, xn, o3, S);
 }
 
 // one pqr segment (cell.h:1511-1693) into the global J, FP64 atomics
@@ -375,6 +419,29 @@ __device__ __forceinline__ void split_rev(const Split &S, const double xo[3], co
 __device__ __forceinline__ double reflect_g(double x, double xm) {
     return (x > xm) * (x - xm) + (x < 0.0) * (xm + x) + (x > 0 && x < xm) * x;
 }
+// reflect_g as a choice (0 keep, 1 subtract xm, 2 add xm, 3 the x == xm case: 0)
+// and its application; apply_wrap(x, xm, wrap_choice(x, xm)) == reflect_g(x, xm)
+__device__ __forceinline__ int wrap_choice(double x, double xm) {
+    return x > xm ? 1 : (x < 0.0 ? 2 : (x == xm ? 3 : 0));
+}
+__device__ __forceinline__ double apply_wrap(double x, double xm, int w) {
+    return w == 1 ? x - xm : (w == 2 ? xm + x : (w == 3 ? 0.0 : x));
+}
+
+// Frozen branches.  Per particle and step, the discrete choices of the flat
+// FP64 push, 16 bits per axis d at bit 16 d: tap indices tn-1, tc-1, the
+// integer parts nI - c_d and cI - c_d of the interpolation weights (c the
+// cell index), the zigzag cell-centre indices i1-1 and i2-1, the periodic
+// wrap and the cell move + 1, 2 bits each.  A forward that replays them is a
+// smooth function of the initial state near the recorded run, and it is the
+// map the adjoint differentiates, so its finite differences check the
+// adjoint without the kinks and jumps of the deposit.
+constexpr unsigned ST_BRANCH_RANGE = 64u;  // a choice outside its 2-bit field (recording)
+__device__ __forceinline__ bool pack2(unsigned long long &code, int v, int shift) {
+    code |= (unsigned long long)(v & 3) << shift;
+    return v >= 0 && v <= 3;
+}
+__device__ __forceinline__ int unpack2(unsigned long long code, int shift) { return (int)((code >> shift) & 3ull); }
 // receivers of a departing particle along one axis (GPU_ArrangeFlights, kernels.cu:316-370)
 // (count of receiving cells along one axis; `first` = the first of them)
 __device__ __forceinline__ int receivers_g(double x, int c, int N, double h, int &first) {
@@ -434,8 +501,26 @@ __global__ void __launch_bounds__(kT) k_flat_push_plain(FlatParams P) {
         g.cell_ijk(cell, i, l, k);
         double x[3] = {S.v[0][j], S.v[1][j], S.v[2][j]};
         double p[3] = {S.v[3][j], S.v[4][j], S.v[5][j]};
+        const int c3[3] = {i, l, k};
+        const unsigned long long rc = P.bmode == 2 ? P.branch[idx] : 0ull;
+        unsigned long long code = 0ull;
+        bool inrange = true;
+        TapInts TI;
+        if (P.bmode == 2) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                TI.tn[d] = unpack2(rc, 16 * d) + 1;
+                TI.tc[d] = unpack2(rc, 16 * d + 2) + 1;
+                TI.nI[d] = unpack2(rc, 16 * d + 4) + c3[d];
+                TI.cI[d] = unpack2(rc, 16 * d + 6) + c3[d];
+            }
+        } else {
+            tap_ints(g, i, l, k, x, TI);
+        }
+        Taps TT;
+        taps_from(g, x, TI, TT);
         double F[6];
-        if (!gather_fields(g, P.E, P.H, i, l, k, x, F)) bad |= ST_STENCIL;
+        if (!gather_fields_taps(g, P.E, P.H, i, l, k, x, TT, F, P.bmode != 2)) bad |= ST_STENCIL;
         if (P.Fout[0]) {
 #pragma unroll
             for (int c = 0; c < 6; c++) P.Fout[c][idx] = F[c];
@@ -445,16 +530,64 @@ __global__ void __launch_bounds__(kT) k_flat_push_plain(FlatParams P) {
         if (!(isfinite(B.pp[0]) && isfinite(B.pp[1]) && isfinite(B.pp[2]))) bad |= ST_NAN;
         const double o3[3] = {(double)i * g.hx, (double)l * g.hy, (double)k * g.hz};
         Split SP;
-        split_plain(g, x, B.x1, o3, SP);
+        if (P.bmode == 2) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                SP.i1[d] = unpack2(rc, 16 * d + 8) + 1;
+                SP.i2[d] = unpack2(rc, 16 * d + 10) + 1;
+            }
+        } else {
+            split_ints(g, x, B.x1, o3, SP);
+        }
+        split_from(g, x, B.x1, o3, SP);
         if (SP.m >= 1 && SP.m <= 7) {
             seg_plain(P.J, g, i, l, k, SP.i1, x, SP.x2, S.m, o3, bad);
             seg_plain(P.J, g, i, l, k, SP.i2, SP.x2, B.x1, S.m, o3, bad);
         } else {
             seg_plain(P.J, g, i, l, k, SP.i1, x, B.x1, S.m, o3, bad);
         }
-        double xr[3] = {reflect_g(B.x1[0], g.lx), reflect_g(B.x1[1], g.ly), reflect_g(B.x1[2], g.lz)};
+        const double L3[3] = {g.lx, g.ly, g.lz};
+        const int n3[3] = {g.nx, g.ny, g.nz};
+        int wr[3];
+        double xr[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            wr[d] = P.bmode == 2 ? unpack2(rc, 16 * d + 12) : wrap_choice(B.x1[d], L3[d]);
+            xr[d] = apply_wrap(B.x1[d], L3[d], wr[d]);
+        }
         const FlatOut &O = P.out[s];
-        O.cell[j] = new_cell_plain(g, cell, i, l, k, xr, amb);
+        int ncell;
+        if (P.bmode == 2) {
+            int r[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                r[d] = c3[d] + unpack2(rc, 16 * d + 14) - 1;
+                r[d] = r[d] < 0 ? r[d] + n3[d] : (r[d] >= n3[d] ? r[d] - n3[d] : r[d]);
+            }
+            ncell = g.cell_of(r[0], r[1], r[2]);
+        } else {
+            ncell = new_cell_plain(g, cell, i, l, k, xr, amb);
+        }
+        if (P.bmode == 1) {
+            int r[3];
+            g.cell_ijk(ncell, r[0], r[1], r[2]);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                int mv = r[d] - c3[d];
+                mv = mv > 1 ? mv - n3[d] : (mv < -1 ? mv + n3[d] : mv);
+                inrange &= pack2(code, TI.tn[d] - 1, 16 * d);
+                inrange &= pack2(code, TI.tc[d] - 1, 16 * d + 2);
+                inrange &= pack2(code, TI.nI[d] - c3[d], 16 * d + 4);
+                inrange &= pack2(code, TI.cI[d] - c3[d], 16 * d + 6);
+                inrange &= pack2(code, SP.i1[d] - 1, 16 * d + 8);
+                inrange &= pack2(code, SP.i2[d] - 1, 16 * d + 10);
+                inrange &= pack2(code, wr[d], 16 * d + 12);
+                inrange &= pack2(code, mv + 1, 16 * d + 14);
+            }
+            P.branch[idx] = code;
+            if (!inrange) bad |= ST_BRANCH_RANGE;
+        }
+        O.cell[j] = ncell;
         O.v[0][j] = xr[0]; O.v[1][j] = xr[1]; O.v[2][j] = xr[2];
         O.v[3][j] = B.pp[0]; O.v[4][j] = B.pp[1]; O.v[5][j] = B.pp[2];
     }
@@ -846,6 +979,28 @@ __global__ void k_flat_gather_plain(SpeciesView S, const int64_t *__restrict__ d
     }
 }
 
+// p += eps * dp for one species, dp interleaved (px, py, pz) in the order of
+// pic_get_particles (tiles in order, slots in order)
+__global__ void k_perturb_momenta(SpeciesView S, int mixed, const int64_t *__restrict__ d0,
+                                  const double *__restrict__ dp, double eps) {
+    const int t = blockIdx.x;
+    const int start = S.tile_start[t], n = S.tile_count[t];
+    const int64_t base = d0[t];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int slot = start + j;
+        const double *q = dp + 3 * (base + j);
+        if (mixed) {
+            S.fx[slot] = (float)((double)S.fx[slot] + eps * q[0]);
+            S.fy[slot] = (float)((double)S.fy[slot] + eps * q[1]);
+            S.fz[slot] = (float)((double)S.fz[slot] + eps * q[2]);
+        } else {
+            S.px[slot] += eps * q[0];
+            S.py[slot] += eps * q[1];
+            S.pz[slot] += eps * q[2];
+        }
+    }
+}
+
 // d_drift and d_vth partial sums: out[0..2] += lambda_p, out[3] += lambda_p . (p - drift)
 __global__ void k_param_grads(int64_t n, const double *__restrict__ lpx, const double *__restrict__ lpy,
                               const double *__restrict__ lpz, const double *__restrict__ px,
@@ -947,6 +1102,8 @@ FlatParams flat_params(pic_handle *h, AdjState &A, char *state, void *const F[PI
         for (int a = 0; a < 6; a++) P.out[s].v[a] = (double *)v[s][a];
     }
     P.st = A.st;
+    P.branch = A.step_branch;
+    P.bmode = A.step_branch ? A.step_bmode : 0;
     return P;
 }
 
@@ -1004,6 +1161,8 @@ int check_adj_status(pic_handle *h, AdjState &A, const char *where) {
     CK(cudaStreamSynchronize(h->stream), "sync");
     A.ambiguous = st.ambiguous;
     if (st.flags & ST_NAN) return set_err(h, PIC_ERR_NAN, "non-finite momentum in the differentiable run");
+    if (st.flags & ST_BRANCH_RANGE)
+        return set_err(h, PIC_ERR_STATE, "branch recording: a discrete choice outside its recorded range");
     if (st.flags & ST_STENCIL) {
         char msg[160];
         snprintf(msg, sizeof(msg), "%s: a particle moved more than half a cell in one step", where);
@@ -1032,7 +1191,7 @@ void adj_free(pic_handle *h) {
     if (!h || !h->adj) return;
     AdjState *A = h->adj;
     void *bufs[] = {A->cur, A->ckp, A->ckf, A->segp, A->segf, A->subp, A->subf, A->lamp, A->lamf, A->rf, A->ha,
-                    A->hist, A->st, A->red, A->lamF, A->segF};
+                    A->hist, A->st, A->red, A->lamF, A->segF, A->branch};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (A->e0) cudaEventDestroy(A->e0);
@@ -1126,7 +1285,17 @@ int forward_run(pic_handle *h, AdjState &A) {
                 CK(cudaMemcpyAsync(A.ckf + ((size_t)c * 6 + a) * fbytes, h->f[PIC_EX + a], fbytes,
                                    cudaMemcpyDeviceToDevice, st), "ckpt fields");
         }
+        const size_t np_all = (size_t)total_particles(A);
+        if (A.branch_mode == 1) {
+            A.step_branch = A.branch + (size_t)n * np_all;
+            A.step_bmode = 1;
+        } else if (A.branch_mode == 2) {
+            A.step_branch = const_cast<unsigned long long *>(A.branch_src) + (size_t)n * np_all;
+            A.step_bmode = 2;
+        }
         int rc = flat_step(h, A, A.cur, h->f, nullptr, nullptr);
+        A.step_branch = nullptr;
+        A.step_bmode = 0;
         if (rc) return rc;
         if (h->mixed)
             k_history<float><<<node_grid(g), 32, 0, st>>>(g, (const float *)h->f[PIC_EX], (const float *)h->f[PIC_EY],
@@ -1306,7 +1475,9 @@ extern "C" {
 
 int pic_forward(pic_handle *h, int steps, int ckpt_every) { return pic_forward2(h, steps, ckpt_every, ckpt_every); }
 
-int pic_forward2(pic_handle *h, int steps, int ckpt_every, int sub_every) {
+// pic_forward2, or (src != null) a forward that replays the discrete choices
+// recorded by src's last forward
+static int forward_impl(pic_handle *h, int steps, int ckpt_every, int sub_every, const pic_handle *src) {
     if (!h) return PIC_ERR_ARG;
     if (steps < 1 || ckpt_every < 1) return set_err(h, PIC_ERR_ARG, "pic_forward: steps and ckpt_every must be >= 1");
     if (sub_every < 1 || sub_every > ckpt_every)
@@ -1335,6 +1506,23 @@ int pic_forward2(pic_handle *h, int steps, int ckpt_every, int sub_every) {
     }
     A.pbytes = adj_state_bytes(A);
     const size_t fbytes = g.nodes_pitched() * (h->mixed ? sizeof(float) : sizeof(double));
+    if (src) {
+        const AdjState *S = src->adj;
+        bool same = S && S->branch && !h->mixed && S->nsp == A.nsp && S->steps >= steps;
+        for (int s = 0; same && s < A.nsp; s++) same = S->n[s] == A.n[s];
+        if (!same)
+            return set_err(h, PIC_ERR_ARG,
+                           "pic_forward_replay: the source needs a recorded FP64 forward of at least as many steps "
+                           "and the same particle counts");
+        A.branch_mode = 2;
+        A.branch_src = S->branch;
+    } else if (h->branch_record && !h->mixed) {
+        if ((rc = adj_alloc(h, (void **)&A.branch,
+                            (size_t)steps * (size_t)total_particles(A) * sizeof(unsigned long long),
+                            "the branch record")))
+            return rc;
+        A.branch_mode = 1;
+    }
     CK(cudaEventCreate(&A.e0), "event");
     CK(cudaEventCreate(&A.e1), "event");
     if ((rc = adj_alloc(h, (void **)&A.cur, A.pbytes, "the particle state"))) return rc;
@@ -1392,6 +1580,58 @@ int pic_forward2(pic_handle *h, int steps, int ckpt_every, int sub_every) {
     h->kin_valid = 0;
     A.have_forward = 1;
     return PIC_OK;
+}
+
+int pic_forward2(pic_handle *h, int steps, int ckpt_every, int sub_every) {
+    return forward_impl(h, steps, ckpt_every, sub_every, nullptr);
+}
+
+int pic_branch_record(pic_handle *h, int on) {
+    if (!h) return PIC_ERR_ARG;
+    if (on && h->mixed) return set_err(h, PIC_ERR_ARG, "pic_branch_record: the FP64 plain form only");
+    h->branch_record = on ? 1 : 0;
+    return PIC_OK;
+}
+
+int pic_perturb_momenta(pic_handle *h, int species, int64_t n, const double *dp, double eps) {
+    if (!h || species < 0 || species >= h->cfg.nspecies || n < 0 || (n > 0 && !dp))
+        return set_err(h, PIC_ERR_ARG, "bad argument");
+    int rc = set_device(h);
+    if (rc) return rc;
+    if ((rc = need_particles(h))) return rc;
+    const Grid &g = h->g;
+    std::vector<int> counts;
+    if ((rc = tile_counts(h, species, counts))) return rc;
+    std::vector<int64_t> d0(g.ntiles + 1);
+    int64_t acc = 0;
+    for (int t = 0; t < g.ntiles; t++) { d0[t] = acc; acc += counts[t]; }
+    d0[g.ntiles] = acc;
+    if (acc != n) return set_err(h, PIC_ERR_ARG, "pic_perturb_momenta: n is not the species' particle count");
+    if (n == 0) return PIC_OK;
+    int64_t *dd = nullptr;
+    double *dv = nullptr;
+    CK(cudaMalloc(&dd, (g.ntiles + 1) * sizeof(int64_t)), "alloc");
+    cudaError_t e = cudaMalloc(&dv, (size_t)n * 3 * sizeof(double));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dd, d0.data(), (g.ntiles + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dv, dp, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        k_perturb_momenta<<<g.ntiles, 256, 0, h->stream>>>(h->sp[species].v, h->mixed, dd, dv, eps);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dd);
+    if (dv) cudaFree(dv);
+    CK(e, "perturb momenta");
+    h->kin_valid = 0;
+    return PIC_OK;
+}
+
+int pic_forward_replay(pic_handle *h, int steps, const pic_handle *recorded) {
+    if (!h || !recorded) return PIC_ERR_ARG;
+    if (h->mixed) return set_err(h, PIC_ERR_ARG, "pic_forward_replay: the FP64 plain form only");
+    return forward_impl(h, steps, steps, steps, recorded);
 }
 
 int pic_forward_history(pic_handle *h, double *out) {

@@ -45,6 +45,14 @@ struct AdjState {
     char *rf;          // field set of the recompute (form's layout: 12 arrays)
     char *ha;          // B after the half step of the step being reversed (3 arrays)
     double *hist;      // steps x 3: sum over nodes 1..N of E_c^2 after each step
+    // frozen branches (plain form): mode 1 records every step's discrete
+    // choices into branch (steps x particles codes), mode 2 replays those of
+    // branch_src; step_branch / step_bmode are what the next flat push uses
+    unsigned long long *branch;
+    const unsigned long long *branch_src;
+    int branch_mode;
+    unsigned long long *step_branch;
+    int step_bmode;
     double *red;       // reduction scratch
     AdjStatus *st;
     std::vector<double> hhist;  // host copy of hist x cell volume

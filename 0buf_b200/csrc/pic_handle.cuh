@@ -54,6 +54,7 @@ struct pic_handle {
     // rho, the Gauss residual G = div E - rho and its stored baseline
     double *rho, *gauss, *gauss0;
     int gauss_has_base;
+    int branch_record;  // the next pic_forward records its discrete choices (pic_branch_record)
 };
 
 namespace pic_host {

@@ -244,6 +244,20 @@ class PicSimulation:
             self._ck(self.lib.pic_forward2(self.h, int(steps), int(ckpt_every), int(sub_every)), "pic_forward2")
         self._fwd_steps = int(steps)
 
+    def branch_record(self, on: bool = True):
+        """``pic_branch_record``: the next forward (FP64) records its discrete choices."""
+        self._ck(self.lib.pic_branch_record(self.h, int(bool(on))), "pic_branch_record")
+
+    def forward_replay(self, steps: int, recorded: "PicSimulation"):
+        """``pic_forward_replay``: forward that replays ``recorded``'s choices (frozen branches)."""
+        self._ck(self.lib.pic_forward_replay(self.h, int(steps), recorded.h), "pic_forward_replay")
+        self._fwd_steps = int(steps)
+
+    def perturb_momenta(self, species: int, dp: np.ndarray, eps: float):
+        """``pic_perturb_momenta``: p += eps * dp, dp (n, 3) in ``particles(species)`` order."""
+        a = np.ascontiguousarray(dp, dtype=np.float64).reshape(-1, 3)
+        self._ck(self.lib.pic_perturb_momenta(self.h, species, a.shape[0], dptr(a), float(eps)), "pic_perturb_momenta")
+
     def history(self) -> np.ndarray:
         """(steps, 3): h^3 * sum over nodes 1..N of E_c^2 after each step of the last forward run."""
         out = np.zeros((self._fwd_steps, 3))

@@ -441,6 +441,49 @@ def run_adjoint(args, pkg, dev):
             fd[form][k] = [float(f"{x:.3e}") for x in v] if isinstance(v, list) else float(f"{v:.3e}")
     out["fd_check"] = {"reference": "FP64 central differences of the FP64 forward", "fd_drift": d_drift,
                        "fd_vth": d_vth, **fd}
+    out["fd_frozen"] = frozen_branch_check(pkg, cfg, dev, steps, base, grads)
+    return out
+
+
+def frozen_branch_check(pkg, cfg, dev, steps, base, grads):
+    """Exact check of the adjoints along dense directions: FP64 central
+    differences (eps 1e-6) of a forward that replays the discrete choices of
+    a recorded FP64 run (pic_branch_record / pic_forward_replay) -- smooth in
+    the initial momenta and the map pic_backward differentiates -- along the
+    thermal spread, the drift and a random direction over every beam particle."""
+    import numpy as np
+    rec = make_sim(pkg, cfg, "fp64", dev, 0)
+    rec.branch_record(True)
+    rec.forward(steps, steps)
+    l_rec = rec.loss_value(field="Ex", window=ADJ_LOSS["window"])
+    sp = ADJ_LOSS["species"]
+
+    def loss(dp, eps):
+        s = make_sim(pkg, cfg, "fp64", dev, 0)
+        if eps:
+            s.perturb_momenta(sp, dp, eps)
+        s.forward_replay(steps, rec)
+        v = s.loss_value(field="Ex", window=ADJ_LOSS["window"])
+        s.close()
+        return v
+
+    n = base["x"].size
+    xi = np.stack([base["px"] - ADJ_LOSS["drift"][0], base["py"], base["pz"]], axis=1) / ADJ_LOSS["vth"]
+    e_x = np.zeros((n, 3))
+    e_x[:, 0] = 1.0
+    dirs = {"vth": xi, "drift_x": e_x, "dense_random": np.random.default_rng(17).standard_normal((n, 3))}
+    out = {"reference": "FP64 central differences, eps 1e-6, of the forward replaying a recorded FP64 run's "
+                        "discrete choices (taps, zigzag split classes, wraps, cell moves)",
+           "replay_at_eps0_rel_diff": float(f"{abs(loss(None, 0.0) - l_rec) / abs(l_rec):.3e}")}
+    eps = 1e-6
+    for name, dp in dirs.items():
+        fd = (loss(dp, eps) - loss(dp, -eps)) / (2 * eps)
+        out[name] = {"fd": fd}
+        for form in ("fp64", "fp32"):
+            ad = float(np.sum(grads[form]["d_p0"] * dp))
+            out[name][f"{form}_adjoint"] = ad
+            out[name][f"{form}_rel_err"] = float(f"{abs(ad - fd) / abs(fd):.3e}")
+    rec.close()
     return out
 
 

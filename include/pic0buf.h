@@ -268,6 +268,25 @@ int pic_forward(pic_handle *h, int steps, int ckpt_every);
  * particle states instead of steps/ckpt_every + ckpt_every + 1, for one more
  * forward recomputation.  sub_every = ckpt_every is pic_forward. */
 int pic_forward2(pic_handle *h, int steps, int ckpt_every, int sub_every);
+/* Exact checks of the adjoint (no counterpart in the reference).  The
+ * deposit's zigzag split and the interpolation's tap choice make L only
+ * piecewise smooth, so plain finite differences along dense directions are
+ * limited by kinks and jumps.  With pic_branch_record(h, 1) the next
+ * pic_forward / pic_forward2 of h (FP64 plain form) records every discrete
+ * choice of every particle and step (tap indices, the integer parts of the
+ * interpolation weights, the cell-centre indices of the zigzag split, the
+ * periodic wraps and the cell moves: 8 bytes per particle-step, kept until
+ * pic_adjoint_free / the next pic_forward / pic_destroy).
+ * pic_forward_replay(h, steps, rec) runs a forward of h (no checkpoints)
+ * that replays rec's recorded choices: a smooth function of the initial
+ * state near rec's run, equal to it at the same state, and exactly the map
+ * pic_backward differentiates.  h must hold the same particle counts per
+ * species in the same order (same generator and seed).
+ * pic_perturb_momenta adds eps * dp to the momenta of one species; dp holds
+ * 3*n doubles (px, py, pz) in pic_get_particles order. */
+int pic_branch_record(pic_handle *h, int on);
+int pic_forward_replay(pic_handle *h, int steps, const pic_handle *recorded);
+int pic_perturb_momenta(pic_handle *h, int species, int64_t n, const double *dp, double eps);
 /* out[n*3 + c] = W[n][c] of the last forward run (host array of 3*steps) */
 int pic_forward_history(pic_handle *h, double *out);
 int pic_loss_value(pic_handle *h, const pic_loss *loss, double *value);

@@ -161,3 +161,39 @@ def test_mixed_gradient_matches_fp64(pkg):
     e_x[:, 0] = 1.0
     fd = fd_along(pkg, base, e_x, eps=1e-8)
     assert abs(g32["d_drift"][0] - fd) / abs(fd) < 1e-3
+
+
+def test_frozen_branch_differences_match_adjoint(pkg):
+    """Exact check of the adjoint along dense directions.  A forward that
+    replays the recorded run's discrete choices (pic_forward_replay) is a
+    smooth function of the initial momenta and the very map pic_backward
+    differentiates; its central differences at eps 1e-6 must match the
+    adjoint to differencing accuracy along the thermal spread, the drift and
+    a random direction over every beam particle.  At eps = 0 the replay
+    reproduces the recorded loss."""
+    with make(pkg) as base:
+        p0 = base.particles(BEAM)
+        base.branch_record(True)
+        base.forward(STEPS, 7)
+        g = base.backward(**LOSS)
+        n = p0["x"].size
+
+        def loss(dp, eps):
+            with make(pkg) as s:
+                if eps:
+                    s.perturb_momenta(BEAM, dp, eps)
+                s.forward_replay(STEPS, base)
+                return s.loss_value(field="Ex", window=WINDOW)
+
+        assert abs(loss(None, 0.0) - g["loss"]) <= 1e-12 * abs(g["loss"])
+        xi = np.stack([p0["px"] - 0.2, p0["py"], p0["pz"]], axis=1) / 0.002
+        e_x = np.zeros((n, 3))
+        e_x[:, 0] = 1.0
+        dirs = {"vth": xi, "drift": e_x, "dense": np.random.default_rng(7).standard_normal((n, 3))}
+        errs = {}
+        for name, dp in dirs.items():
+            eps = 1e-6
+            fd = (loss(dp, eps) - loss(dp, -eps)) / (2 * eps)
+            ad = float(np.sum(g["d_p0"] * dp))
+            errs[name] = abs(fd - ad) / abs(ad)
+        assert max(errs.values()) < 1e-6, errs
