@@ -22,10 +22,10 @@ constexpr float kOneBelow = 0.99999994f;  // largest float < 1
 __global__ void k_b_half_mixed(Grid g, const float *__restrict__ Ex, const float *__restrict__ Ey,
                                const float *__restrict__ Ez, float *Hx, float *Hy, float *Hz, float cx, float cy,
                                float cz) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int l = blockIdx.y;
-    int i = blockIdx.z;
-    if (k >= g.NZ) return;
+    // one thread per node of an x plane (l, k flattened: no idle z tail)
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NY * g.NZ) return;
+    const int l = q / g.NZ, k = q - l * g.NZ, i = blockIdx.y;
     size_t n = g.node(i, l, k);
     size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
     if (i <= g.nx + 1 && l <= g.ny && k <= g.nz) Hx[n] += 0.5f * (cz * (Ey[n + 1] - Ey[n]) - cy * (Ez[n + sy] - Ez[n]));
@@ -38,10 +38,10 @@ __global__ void k_e_update_mixed(Grid g, float *Ex, float *Ey, float *Ez, const 
                                  const float *__restrict__ Hy, const float *__restrict__ Hz,
                                  const double *__restrict__ Jx, const double *__restrict__ Jy,
                                  const double *__restrict__ Jz, float cx, float cy, float cz, double tau) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int l = blockIdx.y;
-    int i = blockIdx.z;
-    if (k >= g.NZ) return;
+    // one thread per node of an x plane (l, k flattened: no idle z tail)
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NY * g.NZ) return;
+    const int l = q / g.NZ, k = q - l * g.NZ, i = blockIdx.y;
     size_t n = g.node(i, l, k);
     size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
     if (i <= g.nx && l >= 1 && l <= g.ny && k >= 1 && k <= g.nz)
@@ -569,18 +569,19 @@ __global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
 
 }  // namespace
 
-static inline dim3 node_grid(const Grid &g, int bx) { return dim3((g.NZ + bx - 1) / bx, g.NY, g.NX); }
+constexpr int kPlaneThreads = 256;
+static inline dim3 plane_grid(const Grid &g) {
+    return dim3((g.NY * g.NZ + kPlaneThreads - 1) / kPlaneThreads, g.NX);
+}
 
 void yee_b_half_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s) {
     float cx = (float)(g.tau / g.hx), cy = (float)(g.tau / g.hy), cz = (float)(g.tau / g.hz);
-    int bx = g.NZ >= 128 ? 128 : 32;
-    k_b_half_mixed<<<node_grid(g, bx), bx, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], cx, cy, cz);
+    k_b_half_mixed<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], cx, cy, cz);
 }
 
 void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], double *const J[3], cudaStream_t s) {
     float cx = (float)(g.tau / g.hx), cy = (float)(g.tau / g.hy), cz = (float)(g.tau / g.hz);
-    int bx = g.NZ >= 128 ? 128 : 32;
-    k_e_update_mixed<<<node_grid(g, bx), bx, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], J[0], J[1], J[2], cx,
+    k_e_update_mixed<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], J[0], J[1], J[2], cx,
                                                      cy, cz, g.tau);
 }
 

@@ -22,10 +22,10 @@ namespace {
 __global__ void k_b_half_plain(Grid g, const double *__restrict__ Ex, const double *__restrict__ Ey,
                                const double *__restrict__ Ez, double *Hx, double *Hy, double *Hz, double *Qx,
                                double *Qy, double *Qz, double cx, double cy, double cz) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int l = blockIdx.y;
-    int i = blockIdx.z;
-    if (k >= g.NZ) return;
+    // one thread per node of an x plane (l, k flattened: no idle z tail)
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NY * g.NZ) return;
+    const int l = q / g.NZ, k = q - l * g.NZ, i = blockIdx.y;
     size_t n = g.node(i, l, k);
     size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
     if (i <= g.nx + 1 && l <= g.ny && k <= g.nz) {
@@ -51,10 +51,10 @@ __global__ void k_b_half_plain(Grid g, const double *__restrict__ Ex, const doub
 // emh2_Element (kernels.cu:1024-1049) over the same ranges
 __global__ void k_b_complete_plain(Grid g, double *Hx, double *Hy, double *Hz, const double *__restrict__ Qx,
                                    const double *__restrict__ Qy, const double *__restrict__ Qz) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int l = blockIdx.y;
-    int i = blockIdx.z;
-    if (k >= g.NZ) return;
+    // one thread per node of an x plane (l, k flattened: no idle z tail)
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NY * g.NZ) return;
+    const int l = q / g.NZ, k = q - l * g.NZ, i = blockIdx.y;
     size_t n = g.node(i, l, k);
     if (i <= g.nx + 1 && l <= g.ny && k <= g.nz) Hx[n] += Qx[n];
     if (i <= g.nx && l <= g.ny + 1 && k <= g.nz) Hy[n] += Qy[n];
@@ -70,10 +70,10 @@ __global__ void k_e_update_plain(Grid g, double *Ex, double *Ey, double *Ez, con
                                  const double *__restrict__ Hy, const double *__restrict__ Hz,
                                  const double *__restrict__ Jx, const double *__restrict__ Jy,
                                  const double *__restrict__ Jz, double cx, double cy, double cz, double tau) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int l = blockIdx.y;
-    int i = blockIdx.z;
-    if (k >= g.NZ) return;
+    // one thread per node of an x plane (l, k flattened: no idle z tail)
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NY * g.NZ) return;
+    const int l = q / g.NZ, k = q - l * g.NZ, i = blockIdx.y;
     size_t n = g.node(i, l, k);
     size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
     if (i <= g.nx && l >= 1 && l <= g.ny && k >= 1 && k <= g.nz)
@@ -507,26 +507,26 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
 }  // namespace
 
 // ------------------------------------------------------------ launchers --
-static inline dim3 node_grid(const Grid &g, int bx) { return dim3((g.NZ + bx - 1) / bx, g.NY, g.NX); }
+constexpr int kPlaneThreads = 256;
+static inline dim3 plane_grid(const Grid &g) {
+    return dim3((g.NY * g.NZ + kPlaneThreads - 1) / kPlaneThreads, g.NX);
+}
 
 void yee_b_half_plain(const Grid &g, double *const F[12], cudaStream_t s) {
     // getMagneticFieldTimeMeshFactors, gpu_plasma.h:512-522
     double cx = g.tau / (g.hx), cy = g.tau / (g.hy), cz = g.tau / g.hz;
-    int bx = g.NZ >= 128 ? 128 : 32;
-    k_b_half_plain<<<node_grid(g, bx), bx, 0, s>>>(g, F[PIC_EX], F[PIC_EY], F[PIC_EZ], F[PIC_HX], F[PIC_HY],
+    k_b_half_plain<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, F[PIC_EX], F[PIC_EY], F[PIC_EZ], F[PIC_HX], F[PIC_HY],
                                                    F[PIC_HZ], F[PIC_QX], F[PIC_QY], F[PIC_QZ], cx, cy, cz);
 }
 
 void yee_b_complete_plain(const Grid &g, double *const F[12], cudaStream_t s) {
-    int bx = g.NZ >= 128 ? 128 : 32;
-    k_b_complete_plain<<<node_grid(g, bx), bx, 0, s>>>(g, F[PIC_HX], F[PIC_HY], F[PIC_HZ], F[PIC_QX],
+    k_b_complete_plain<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, F[PIC_HX], F[PIC_HY], F[PIC_HZ], F[PIC_QX],
                                                        F[PIC_QY], F[PIC_QZ]);
 }
 
 void yee_e_update_plain(const Grid &g, double *const F[12], cudaStream_t s) {
     double cx = g.tau / (g.hx), cy = g.tau / (g.hy), cz = g.tau / g.hz;
-    int bx = g.NZ >= 128 ? 128 : 32;
-    k_e_update_plain<<<node_grid(g, bx), bx, 0, s>>>(g, F[PIC_EX], F[PIC_EY], F[PIC_EZ], F[PIC_HX],
+    k_e_update_plain<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, F[PIC_EX], F[PIC_EY], F[PIC_EZ], F[PIC_HX],
                                                      F[PIC_HY], F[PIC_HZ], F[PIC_JX], F[PIC_JY], F[PIC_JZ],
                                                      cx, cy, cz, g.tau);
 }
