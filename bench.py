@@ -369,7 +369,11 @@ def run_adjoint(args, pkg, dev):
     uses the median of three small eps for the same reason."""
     import numpy as np
     cfg = dict(pkg.configs.CONFIGS["c3"])
-    steps, K = cfg["steps"], 25
+    if args.adjoint_cells:
+        cfg["cells"] = tuple(int(c) for c in args.adjoint_cells.split(","))
+    if args.adjoint_ppc:
+        cfg["ppc"] = args.adjoint_ppc
+    steps, K = (args.adjoint_steps or cfg["steps"]), 25
     out = {"config": f"c3: {'x'.join(map(str, cfg['cells']))} cells, {cfg['ppc']} particles/cell/species x 3, "
                      f"{steps} steps, checkpoints every {K}, loss = sum over the last 50 steps of h^3 sum E_x^2, "
                      "gradient w.r.t. the beam's initial momenta, drift and thermal spread"}
@@ -403,6 +407,8 @@ def run_adjoint(args, pkg, dev):
             sim.close()
         return (vals[0] - vals[1]) / (2 * eps)
 
+    if args.no_fd:
+        return out
     n = base["x"].size
     # run-to-run spread of L (FP64 atomics add the current in no fixed order)
     sim = make_sim(pkg, cfg, "fp64", dev, 0)
@@ -704,7 +710,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--stress-adjoint", action="store_true",
                     help="also run the stress configuration's differentiable run at full size (FP32, two checkpoint levels)")
-    ap.add_argument("--no-fd", action="store_true", help="skip the finite-difference reference of --stress-adjoint")
+    ap.add_argument("--no-fd", action="store_true",
+                    help="skip the finite-difference checks of the differentiable runs (timings only)")
+    ap.add_argument("--adjoint-steps", type=int, default=0,
+                    help="steps of the adjoint configuration's run (default: its 300; shorter for profiling)")
+    ap.add_argument("--adjoint-cells", default=None, help="override the adjoint configuration's cells (profiling)")
+    ap.add_argument("--adjoint-ppc", type=int, default=0, help="override its particles per cell (profiling)")
     ap.add_argument("--accuracy-steps", type=int, default=0,
                     help="also run both forms this many steps with energies every step (FP32 error history)")
     ap.add_argument("--reference-inner", type=int, default=20)
