@@ -7,7 +7,7 @@ host-side mirror of the reference's step driver over that ABI.
 """
 from . import _capi, configs, compare
 from ._capi import PicError, load as load_library, LIB_PATH
-from .plasma import PicSimulation, Plasma, host_species, profile_counts
+from .plasma import PicSimulation, Plasma, host_species, profile_counts, mumu_name, mumu_read, mumu_write
 
-__all__ = ["PicSimulation", "Plasma", "PicError", "host_species", "profile_counts", "load_library", "LIB_PATH",
-           "configs", "compare"]
+__all__ = ["PicSimulation", "Plasma", "PicError", "host_species", "profile_counts", "mumu_name", "mumu_read",
+           "mumu_write", "load_library", "LIB_PATH", "configs", "compare"]

@@ -56,6 +56,14 @@ class PicGrads(C.Structure):
                 ("d_p0", C.c_void_p), ("reserved", C.c_double * 4)]
 
 
+class PicMumu(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nsort", C.c_int),
+                ("fields", C.c_void_p * 12),
+                ("count", C.c_int64 * PIC_MAX_SPECIES),
+                ("q_m", C.c_double * PIC_MAX_SPECIES), ("m", C.c_double * PIC_MAX_SPECIES),
+                ("p", (C.c_void_p * 6) * PIC_MAX_SPECIES)]
+
+
 class PicProfile(C.Structure):
     _fields_ = [("ppc_mean", C.c_double), ("cos_amp", C.c_double), ("bump_peak", C.c_double),
                 ("bump_sigma", C.c_double), ("bump_centre", C.c_double * 3), ("count_seed", C.c_uint64)]
@@ -101,6 +109,12 @@ SIGNATURES = {
     "pic_gauss_residual": (C.c_int, [H, D]),
     "pic_gauss_check": (C.c_int, [H, C.c_int, D]),
     "pic_momentum": (C.c_int, [H, D]),
+    "pic_mumu_name": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_int]),
+    "pic_mumu_write": (C.c_int, [C.c_char_p, C.POINTER(PicMumu)]),
+    "pic_mumu_read_counts": (C.c_int, [C.c_char_p, C.POINTER(PicMumu)]),
+    "pic_mumu_read": (C.c_int, [C.c_char_p, C.POINTER(PicMumu)]),
+    "pic_dump_write": (C.c_int, [H, C.c_char_p]),
+    "pic_dump_read": (C.c_int, [H, C.c_char_p]),
     "pic_profile_counts": (C.c_int, [C.c_int] * 3 + [C.POINTER(PicProfile), I32, I64]),
     "pic_init_species_profile": (C.c_int, [H, C.c_int, C.POINTER(PicProfile)] + [C.c_double] * 4 + [C.c_uint64]),
     "pic_sync": (C.c_int, [H]),

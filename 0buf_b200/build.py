@@ -36,6 +36,7 @@ UNITS = {
     "pic_mixed.cu": [],
     "pic_noalloc.cu": [],
     "pic_diag.cu": ["-fmad=false"],
+    "pic_dump.cu": [],
     "pic_adjoint.cu": ["-fmad=false"],
     "pic_adjoint_mixed.cu": [],
 }

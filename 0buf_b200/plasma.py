@@ -10,6 +10,7 @@ library; this module only moves arguments and arrays.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Sequence
 
 import numpy as np
@@ -195,6 +196,14 @@ class PicSimulation:
         self._ck(self.lib.pic_gauss_residual(self.h, dptr(a)), "pic_gauss_residual")
         return a
 
+    def dump_write(self, path: str):
+        """``pic_dump_write``: checkpoint in the reference's Fortran-record dump format."""
+        self._ck(self.lib.pic_dump_write(self.h, os.fsencode(path)), "pic_dump_write")
+
+    def dump_read(self, path: str):
+        """``pic_dump_read``: resume from a dump (same grid and species)."""
+        self._ck(self.lib.pic_dump_read(self.h, os.fsencode(path)), "pic_dump_read")
+
     def momentum(self) -> np.ndarray:
         """(nspecies, 3) total mechanical momentum sum (m/q_m) p per species, FP64."""
         out = np.zeros(3 * self.nspecies)
@@ -318,6 +327,73 @@ def _host_ptr(a):
 
 def _length(a) -> int:
     return int(a.size if isinstance(a, np.ndarray) else a.numel())
+
+
+FIELD_ORDER = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz", "Qx", "Qy", "Qz")
+_PKEYS = ("x", "y", "z", "px", "py", "pz")
+
+
+def mumu_name(num: int, nt: int) -> str:
+    """The reference's dump file name ``mumu%03d%08d.dat`` (``pic_mumu_name``)."""
+    buf = C.create_string_buffer(64)
+    rc = _capi.load().pic_mumu_name(int(num), int(nt), buf, 64)
+    if rc != 0:
+        raise PicError(rc, "pic_mumu_name")
+    return buf.value.decode()
+
+
+def mumu_write(path: str, cells, fields=None, sorts=()):
+    """``pic_mumu_write``: fields = dict name -> (Nx+2)(Ny+2)(Nz+2) array (missing: zeros);
+    sorts = [dict(q_m, m, x, y, z, px, py, pz)]."""
+    d = _capi.PicMumu()
+    d.nx, d.ny, d.nz = (int(c) for c in cells)
+    keep = []
+    for a, name in enumerate(FIELD_ORDER):
+        if fields is not None and name in fields:
+            arr = np.ascontiguousarray(fields[name], dtype=np.float64).ravel()
+            keep.append(arr)
+            d.fields[a] = arr.ctypes.data
+    d.nsort = len(sorts)
+    for s, sp in enumerate(sorts):
+        d.q_m[s] = float(sp["q_m"])
+        d.m[s] = float(sp["m"])
+        n = None
+        for a, k in enumerate(_PKEYS):
+            arr = np.ascontiguousarray(sp[k], dtype=np.float64).ravel()
+            n = arr.size if n is None else n
+            assert arr.size == n
+            keep.append(arr)
+            d.p[s][a] = arr.ctypes.data
+        d.count[s] = n or 0
+    rc = _capi.load().pic_mumu_write(os.fsencode(path), C.byref(d))
+    if rc != 0:
+        raise PicError(rc, "pic_mumu_write")
+
+
+def mumu_read(path: str, cells):
+    """``pic_mumu_read``: (fields dict, [dict(q_m, m, x, y, z, px, py, pz)])."""
+    lib = _capi.load()
+    d = _capi.PicMumu()
+    d.nx, d.ny, d.nz = (int(c) for c in cells)
+    rc = lib.pic_mumu_read_counts(os.fsencode(path), C.byref(d))
+    if rc != 0:
+        raise PicError(rc, "pic_mumu_read_counts")
+    nodes = int(np.prod([c + 2 for c in cells]))
+    fields = {name: np.zeros(nodes) for name in FIELD_ORDER}
+    for a, name in enumerate(FIELD_ORDER):
+        d.fields[a] = fields[name].ctypes.data
+    sorts = []
+    for s in range(d.nsort):
+        sp = {k: np.zeros(int(d.count[s])) for k in _PKEYS}
+        for a, k in enumerate(_PKEYS):
+            d.p[s][a] = sp[k].ctypes.data if sp[k].size else None
+        sorts.append(sp)
+    rc = lib.pic_mumu_read(os.fsencode(path), C.byref(d))
+    if rc != 0:
+        raise PicError(rc, "pic_mumu_read")
+    for s, sp in enumerate(sorts):
+        sp["q_m"], sp["m"] = float(d.q_m[s]), float(d.m[s])
+    return fields, sorts
 
 
 def make_profile(profile: dict):

@@ -316,6 +316,40 @@ int pic_adjoint_free(pic_handle *h);
 int pic_field_energy_noalloc(int nx, int ny, int nz, const double *Ex, const double *Ey, const double *Ez,
                              const double *Hx, const double *Hy, const double *Hz, double *out3, void *stream);
 
+/* The reference's Fortran-record dump ("mumu" file: LoadParticleData,
+ * load_data.cu:308-341; readControlPoint, gpu_plasma.h:1088-1125), used as
+ * the on-disk checkpoint/resume of a handle.  Records are an int32 byte
+ * count, the payload and the count again: 12 field records (Ex Ey Ez Hx Hy
+ * Hz Jx Jy Jz Qx Qy Qz, (Nx+2)(Ny+2)(Nz+2) FP64 in the reference layout),
+ * then per particle sort a record (count, q/m, m) and six records x y z px
+ * py pz (global positions).  A record holds at most 2^31-1 bytes (the
+ * reference reader's int), so a species fits when it has at most
+ * 268,435,455 particles.  The host functions need no GPU. */
+typedef struct pic_mumu {
+    int nx, ny, nz;
+    int nsort;                                /* particle sorts in the file */
+    double *fields[12];                       /* host arrays; NULL: write zeros / skip on read */
+    int64_t count[PIC_MAX_SPECIES];
+    double q_m[PIC_MAX_SPECIES], m[PIC_MAX_SPECIES];
+    double *p[PIC_MAX_SPECIES][6];            /* x y z px py pz, count[s] each; NULL: zeros / skip */
+} pic_mumu;
+/* "mumu%03d%08d.dat" of control point num and step nt (the reference's name) */
+int pic_mumu_name(int num, int nt, char *buf, int cap);
+int pic_mumu_write(const char *path, const pic_mumu *d);
+/* fills nsort, count, q_m and m of d (d->nx, ny, nz set by the caller) and
+ * checks every record marker */
+int pic_mumu_read_counts(const char *path, pic_mumu *d);
+/* reads into the caller's arrays; nsort and count must be those of the file */
+int pic_mumu_read(const char *path, pic_mumu *d);
+/* Checkpoint / resume of a handle through the dump: every species in order,
+ * E, H, J and (plain form) Q; the mixed form writes Q as zeros and its FP32
+ * offsets as FP64 global positions.  pic_dump_read needs the same grid,
+ * species count, q/m and charge weights, replaces every species' particles
+ * and sets the stored fields.  No counterpart in the reference beyond the
+ * format, which it only reads. */
+int pic_dump_write(pic_handle *h, const char *path);
+int pic_dump_read(pic_handle *h, const char *path);
+
 /* Status and errors. */
 int pic_sync(pic_handle *h);
 int pic_last_status(pic_handle *h);

@@ -15,6 +15,7 @@ mkdir -p "$OUT"
 nvcc -std=c++14 -O2 -shared -Xcompiler -fPIC,-fopenmp -Wno-deprecated-gpu-targets -w \
   -gencode arch=compute_100a,code=sm_100a \
   -include "$HERE/ref_shim/surface_shim.h" -I"$REF_DIR" \
-  "$HERE/ref_driver.cu" "$REF_DIR/archAPI.cu" -o "$OUT/libref0buf.so.tmp" -lgomp
+  "$HERE/ref_driver.cu" "$REF_DIR/archAPI.cu" "$REF_DIR/load_data.cu" "$REF_DIR/maxwell.cu" \
+  -o "$OUT/libref0buf.so.tmp" -lgomp
 mv "$OUT/libref0buf.so.tmp" "$OUT/libref0buf.so"
 echo "built $OUT/libref0buf.so"

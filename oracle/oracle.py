@@ -248,3 +248,70 @@ def gauss_residual(Ex, Ey, Ez, rho, cells, h):
     G[I, J, K] = ((E[0][I, J, K] - E[0][0:nx, J, K]) / h[0] + (E[1][I, J, K] - E[1][I, 0:ny, K]) / h[1] +
                   (E[2][I, J, K] - E[2][I, J, 0:nz]) / h[2] - r[I, J, K])
     return G.ravel()
+
+
+# ---------------------------------------------------------------------------
+# The reference's Fortran-record dump (LoadParticleData, load_data.cu:308-341;
+# readFortranBinaryArray, load_data.cu:35-63), restated with numpy, and the
+# reference's own reader from the replay library.
+
+def write_mumu_np(path, cells, fields, sorts):
+    """fields: 12 arrays (Ex..Qz, reference layout); sorts: [(q_m, m, x, y, z, px, py, pz)]."""
+    def rec(f, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        t = np.array([a.nbytes], dtype=np.int32).tobytes()
+        f.write(t + a.tobytes() + t)
+    with open(path, "wb") as f:
+        for a in fields:
+            rec(f, a)
+        for q_m, m, *arrs in sorts:
+            rec(f, np.array([len(arrs[0]), q_m, m], dtype=np.float64))
+            for a in arrs:
+                rec(f, a)
+
+
+def read_mumu_np(path, cells):
+    nodes = int(np.prod([c + 2 for c in cells]))
+    raw = open(path, "rb").read()
+    pos = 0
+
+    def rec():
+        nonlocal pos
+        t = int(np.frombuffer(raw, np.int32, 1, pos)[0])
+        a = np.frombuffer(raw, np.float64, t // 8, pos + 4).copy()
+        assert int(np.frombuffer(raw, np.int32, 1, pos + 4 + t)[0]) == t
+        pos += t + 8
+        return a
+    fields = [rec() for _ in range(12)]
+    assert all(f.size == nodes for f in fields)
+    sorts = []
+    while pos < len(raw):
+        head = rec()
+        sorts.append((head[1], head[2], *[rec() for _ in range(6)]))
+    return fields, sorts
+
+
+def ref_read_mumu(workdir, nt, cells):
+    """The reference's LoadParticleData on mumu000<nt>.dat in workdir (replay
+    library only): [(x, y, z, pu, pv, pw, m, q_m) array per sort] for ion,
+    electron, beam."""
+    lib = RefSim.lib()
+    lib.ref_mumu_load.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_long)]
+    lib.ref_mumu_load.restype = C.c_int
+    lib.ref_mumu_particles.argtypes = [C.c_int, D]
+    lib.ref_mumu_particles.restype = C.c_long
+    counts = (C.c_long * 3)()
+    cwd = os.getcwd()
+    try:
+        os.chdir(workdir)
+        rc = lib.ref_mumu_load(int(nt), *[int(c) for c in cells], counts)
+    finally:
+        os.chdir(cwd)
+    if rc != 0:
+        raise RuntimeError(f"LoadParticleData returned {rc}")
+    out = []
+    for s in range(3):
+        a = np.zeros((max(int(counts[s]), 1), 8))
+        n = lib.ref_mumu_particles(s, a.ctypes.data_as(D))
+        out.append(a[:n])
+    return out

@@ -29,6 +29,7 @@
 #include "gpucell.h"
 #include "add.cu"
 #include "kernels.cu"
+#include "load_data.h"
 
 #include <vector>
 #include <cstring>
@@ -494,6 +495,31 @@ long ref_get_particles(void *h, double *out, int *cell, int *sort, int *directio
         }
     }
     return j;
+}
+
+// The reference's own reader of its Fortran-record dump (LoadParticleData,
+// load_data.cu:308-341): reads mumu000<nt>.dat from the working directory --
+// 12 field records, then the ion, electron and beam sorts.  The particles are
+// kept here for ref_mumu_particles.
+static std::vector<Particle> g_mumu[3];
+
+int ref_mumu_load(int nt, int nx, int ny, int nz, long *counts3) {
+    for (auto &v : g_mumu) v.clear();
+    int rc = LoadParticleData(nt, g_mumu[0], g_mumu[1], g_mumu[2], nx, ny, nz);
+    for (int s = 0; s < 3; s++) counts3[s] = (long)g_mumu[s].size();
+    return rc;
+}
+
+// particle j of sort s as x y z pu pv pw m q_m
+long ref_mumu_particles(int sort, double *out8) {
+    if (sort < 0 || sort > 2) return -1;
+    const std::vector<Particle> &v = g_mumu[sort];
+    for (size_t j = 0; j < v.size(); j++) {
+        const Particle &p = v[j];
+        double *o = out8 + 8 * j;
+        o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = p.pu; o[4] = p.pv; o[5] = p.pw; o[6] = p.m; o[7] = p.q_m;
+    }
+    return (long)v.size();
 }
 
 }  // extern "C"
