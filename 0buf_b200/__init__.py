@@ -7,7 +7,8 @@ host-side mirror of the reference's step driver over that ABI.
 """
 from . import _capi, configs, compare
 from ._capi import PicError, load as load_library, LIB_PATH
-from .plasma import PicSimulation, Plasma, host_species, profile_counts, mumu_name, mumu_read, mumu_write
+from .plasma import (PicSimulation, Plasma, Rnd, host_species, profile_counts, mumu_name, mumu_read, mumu_write,
+                     quiet_params, quiet_start)
 
 __all__ = ["PicSimulation", "Plasma", "PicError", "host_species", "profile_counts", "mumu_name", "mumu_read",
-           "mumu_write", "load_library", "LIB_PATH", "configs", "compare"]
+           "mumu_write", "Rnd", "quiet_params", "quiet_start", "load_library", "LIB_PATH", "configs", "compare"]

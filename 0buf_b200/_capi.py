@@ -64,6 +64,18 @@ class PicMumu(C.Structure):
                 ("p", (C.c_void_p * 6) * PIC_MAX_SPECIES)]
 
 
+class PicRnd(C.Structure):
+    _fields_ = [("ix", C.c_int32), ("iy", C.c_int32), ("iz", C.c_int32), ("store", C.c_double)]
+
+
+class PicQuiet(C.Structure):
+    _fields_ = [("n_ions", C.c_int64), ("tex0", C.c_double), ("tey0", C.c_double), ("tez0", C.c_double),
+                ("Tb", C.c_double), ("rimp", C.c_double), ("rbd", C.c_double), ("ni", C.c_double),
+                ("meh", C.c_int), ("lp", C.c_int), ("beamf", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("beam_lx", C.c_double), ("beam_ly", C.c_double), ("beam_lz", C.c_double)]
+
+
 class PicProfile(C.Structure):
     _fields_ = [("ppc_mean", C.c_double), ("cos_amp", C.c_double), ("bump_peak", C.c_double),
                 ("bump_sigma", C.c_double), ("bump_centre", C.c_double * 3), ("count_seed", C.c_uint64)]
@@ -115,6 +127,12 @@ SIGNATURES = {
     "pic_mumu_read": (C.c_int, [C.c_char_p, C.POINTER(PicMumu)]),
     "pic_dump_write": (C.c_int, [H, C.c_char_p]),
     "pic_dump_read": (C.c_int, [H, C.c_char_p]),
+    "pic_rnd_init": (None, [C.POINTER(PicRnd)]),
+    "pic_rnd_uniform": (C.c_double, [C.POINTER(PicRnd)]),
+    "pic_rnd_gaussian": (C.c_double, [C.POINTER(PicRnd), C.c_double, C.c_double]),
+    "pic_rnd_table": (C.c_int, [D]),
+    "pic_quiet_defaults": (C.c_int, [C.POINTER(PicQuiet)]),
+    "pic_quiet_start": (C.c_int, [C.POINTER(PicQuiet)] + [C.POINTER(C.c_void_p)] * 3 + [I64, D, D]),
     "pic_profile_counts": (C.c_int, [C.c_int] * 3 + [C.POINTER(PicProfile), I32, I64]),
     "pic_init_species_profile": (C.c_int, [H, C.c_int, C.POINTER(PicProfile)] + [C.c_double] * 4 + [C.c_uint64]),
     "pic_sync": (C.c_int, [H]),

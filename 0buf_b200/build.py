@@ -37,6 +37,7 @@ UNITS = {
     "pic_noalloc.cu": [],
     "pic_diag.cu": ["-fmad=false"],
     "pic_dump.cu": [],
+    "pic_quiet.cu": ["-Xcompiler", "-ffp-contract=off"],
     "pic_adjoint.cu": ["-fmad=false"],
     "pic_adjoint_mixed.cu": [],
 }

@@ -97,6 +97,10 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
         int64_t pad = h->cfg.capacity_pad >= 0 ? h->cfg.capacity_pad : 64;
         int64_t cap = (int64_t)counts[t] + (int64_t)ceil(counts[t] * slack) + pad;
         if (pad > 0) cap = (cap + 31) / 32 * 32;
+        // the plain form's two-word tile J stays exact up to kFxMaxTileSlots
+        // particles in a tile over all species
+        if (!h->mixed && cap > kFxMaxTileSlots / h->cfg.nspecies)
+            return set_err(h, PIC_ERR_ARG, "too many particles in one tile for the FP64 tile current");
         acc += cap;
         if (acc > 0x7fffff00LL) return set_err(h, PIC_ERR_ARG, "species capacity exceeds 2^31 slots");
     }

@@ -94,6 +94,31 @@ __device__ __forceinline__ void fx_addf(unsigned long long *a, float v, float in
     long long iv = __float2ll_rn(v * inv_q);
     if (iv) atomicAdd(a, (unsigned long long)iv);
 }
+// Two-word form for the FP64 plain form.  The bound above assumes every
+// particle moves at c; a dense slow plasma (thousands of particles per cell at
+// v ~ 1e-3, whose beam and return currents cancel) adds contributions ~1e-9 of
+// the bound, which a single word rounds at ~1e-10 of their size.  The second
+// word takes each contribution's remainder in units of q * 2^-40:
+//   s = v / q (exact: q is a power of two), r = rint(s), s - r exact
+//   (Sterbenz: |s - r| <= 1/2 and r, s within a factor 2 when r != 0),
+// so the error is <= q * 2^-41 per contribution, and both adds are exact
+// integer adds (order-independent).  |lo| grows by <= 2^39 per add: 2^24
+// adds into one node before it could overflow, i.e. 8M particles in a tile
+// (kFxMaxTileSlots guards it).
+constexpr int kFxLoBits = 40;
+constexpr long long kFxMaxTileSlots = 1ll << 23;
+__device__ __forceinline__ void fx_split(double v, double inv_q, long long &ih, long long &il) {
+    const double s = v * inv_q;
+    const double r = rint(s);
+    ih = (long long)r;
+    il = __double2ll_rn((s - r) * 1099511627776.0);  // 2^40
+}
+__device__ __forceinline__ void fx_add2(unsigned long long *hi, unsigned long long *lo, double v, double inv_q) {
+    long long ih, il;
+    fx_split(v, inv_q, ih, il);
+    if (ih) atomicAdd(hi, (unsigned long long)ih);
+    if (il) atomicAdd(lo, (unsigned long long)il);
+}
 
 struct SpeciesView {
     // plain form

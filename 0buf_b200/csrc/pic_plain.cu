@@ -183,19 +183,20 @@ __device__ __forceinline__ void pqr_plain(unsigned long long *__restrict__ sJ, d
     if (iv[0] < 2 || iv[0] > 3 || iv[1] < 2 || iv[1] > 3 || iv[2] < 2 || iv[2] > 3) { bad |= ST_STENCIL; return; }
     int n = ((bi + iv[0]) * SY + (bl + iv[1])) * SZ + (bk + iv[2]);
     int ez = 1, ey = SZ, ex = SY * SZ;
-    unsigned long long *Jx = sJ, *Jy = sJ + nn, *Jz = sJ + 2 * nn;
-    fx_add(&Jx[n], su * (dy1 * dz1 + s1), inv_q);
-    fx_add(&Jx[n + ez], su * (dy1 * dz - s1), inv_q);
-    fx_add(&Jx[n + ey], su * (dy * dz1 - s1), inv_q);
-    fx_add(&Jx[n + ey + ez], su * (dy * dz + s1), inv_q);
-    fx_add(&Jy[n], sv * (dx1 * dz1 + s2), inv_q);
-    fx_add(&Jy[n + ez], sv * (dx1 * dz - s2), inv_q);
-    fx_add(&Jy[n + ex], sv * (dx * dz1 - s2), inv_q);
-    fx_add(&Jy[n + ex + ez], sv * (dx * dz + s2), inv_q);
-    fx_add(&Jz[n], sw * (dx1 * dy1 + s3), inv_q);
-    fx_add(&Jz[n + ey], sw * (dx1 * dy - s3), inv_q);
-    fx_add(&Jz[n + ex], sw * (dx * dy1 - s3), inv_q);
-    fx_add(&Jz[n + ex + ey], sw * (dx * dy + s3), inv_q);
+    unsigned long long *Jx = sJ, *Jy = sJ + nn, *Jz = sJ + 2 * nn;  // low words at + 3 nn
+    const int lo = 3 * nn;
+    fx_add2(&Jx[n], &Jx[n + lo], su * (dy1 * dz1 + s1), inv_q);
+    fx_add2(&Jx[n + ez], &Jx[n + ez + lo], su * (dy1 * dz - s1), inv_q);
+    fx_add2(&Jx[n + ey], &Jx[n + ey + lo], su * (dy * dz1 - s1), inv_q);
+    fx_add2(&Jx[n + ey + ez], &Jx[n + ey + ez + lo], su * (dy * dz + s1), inv_q);
+    fx_add2(&Jy[n], &Jy[n + lo], sv * (dx1 * dz1 + s2), inv_q);
+    fx_add2(&Jy[n + ez], &Jy[n + ez + lo], sv * (dx1 * dz - s2), inv_q);
+    fx_add2(&Jy[n + ex], &Jy[n + ex + lo], sv * (dx * dz1 - s2), inv_q);
+    fx_add2(&Jy[n + ex + ez], &Jy[n + ex + ez + lo], sv * (dx * dz + s2), inv_q);
+    fx_add2(&Jz[n], &Jz[n + lo], sw * (dx1 * dy1 + s3), inv_q);
+    fx_add2(&Jz[n + ey], &Jz[n + ey + lo], sw * (dx1 * dy - s3), inv_q);
+    fx_add2(&Jz[n + ex], &Jz[n + ex + lo], sw * (dx * dy1 - s3), inv_q);
+    fx_add2(&Jz[n + ex + ey], &Jz[n + ex + ey + lo], sw * (dx * dy + s3), inv_q);
 }
 
 // Reflect, cell.h:1427-1478
@@ -230,8 +231,8 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
     const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
     const int nn = SX * SY * SZ;
     double *sF = (double *)smem_raw;  // Ex Ey Ez Hx Hy Hz
-    unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);  // fixed-point tile J
-    int *sHoles = (int *)(sJ + 3 * nn);
+    unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);  // fixed-point tile J: 3 nn high, 3 nn low words
+    int *sHoles = (int *)(sJ + 6 * nn);
     int *sFront = sHoles + kHoleMax;
     if (threadIdx.x == 0) {
         double bound = 0.0;
@@ -257,9 +258,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
         sF[3 * nn + idx] = in ? H[0][n] : 0.0;
         sF[4 * nn + idx] = in ? H[1][n] : 0.0;
         sF[5 * nn + idx] = in ? H[2][n] : 0.0;
-        sJ[idx] = 0ull;
-        sJ[nn + idx] = 0ull;
-        sJ[2 * nn + idx] = 0ull;
+        for (int w = 0; w < 6; w++) sJ[w * nn + idx] = 0ull;
     }
     __syncthreads();
 
@@ -481,12 +480,13 @@ __global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
 
     // ---- tile J -> global J (GPU_WriteAllCurrents, kernels.cu:83-112)
     for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
-        long long iv = (long long)sJ[idx];
-        if (iv != 0) {
+        const long long ih = (long long)sJ[idx], il = (long long)sJ[3 * nn + idx];
+        if (ih != 0 || il != 0) {
             int comp = idx / nn, r = idx % nn;
             int c = r % SZ, b = (r / SZ) % SY, a = r / (SZ * SY);
             if (i0 + a < g.NX && l0 + b < g.NY && k0 + c < g.NZ)
-                atomicAdd(&P.J[comp][g.node(i0 + a, l0 + b, k0 + c)], (double)iv * sQ);
+                atomicAdd(&P.J[comp][g.node(i0 + a, l0 + b, k0 + c)],
+                          ((double)ih + (double)il * 9.094947017729282e-13) * sQ);  // il * 2^-40
         }
     }
     // ---- kinetic energy and counters
@@ -574,7 +574,7 @@ void e_ghosts_mixed(const Grid &g, float *Ex, float *Ey, float *Ez, int periodic
 
 size_t push_smem_plain(const Grid &g) {
     size_t nn = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2);
-    return 6 * nn * sizeof(double) + 3 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
+    return 6 * nn * sizeof(double) + 6 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
 }
 
 cudaError_t launch_push_plain(const StepParams &p, cudaStream_t s) {

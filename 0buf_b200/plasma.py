@@ -435,6 +435,80 @@ def host_species(cells, lengths, species_index: int, ppc: int, drift=(0.0, 0.0, 
     return arrs
 
 
+class Rnd:
+    """The reference's random numbers (``rnd_uniform`` / ``rnd_gaussian``,
+    maxwell.cu:187-197) with the state held here: ``Rnd()`` starts where the
+    reference starts, ``Rnd(ix, iy, iz, store)`` anywhere else."""
+
+    def __init__(self, ix=None, iy=None, iz=None, store=None):
+        self._lib = _capi.load()
+        self.state = _capi.PicRnd()
+        self._lib.pic_rnd_init(C.byref(self.state))
+        for k, v in (("ix", ix), ("iy", iy), ("iz", iz), ("store", store)):
+            if v is not None:
+                setattr(self.state, k, v)
+
+    def uniform(self, n: int | None = None):
+        if n is None:
+            return self._lib.pic_rnd_uniform(C.byref(self.state))
+        return np.array([self._lib.pic_rnd_uniform(C.byref(self.state)) for _ in range(int(n))])
+
+    def gaussian(self, mean=0.0, sd=1.0, n: int | None = None):
+        if n is None:
+            return self._lib.pic_rnd_gaussian(C.byref(self.state), float(mean), float(sd))
+        return np.array([self._lib.pic_rnd_gaussian(C.byref(self.state), float(mean), float(sd))
+                         for _ in range(int(n))])
+
+    @staticmethod
+    def table() -> np.ndarray:
+        out = np.zeros(41)
+        rc = _capi.load().pic_rnd_table(dptr(out))
+        if rc != 0:
+            raise PicError(rc, "pic_rnd_table")
+        return out
+
+
+QUIET_SORTS = ("ions", "electrons", "beam")
+
+
+def quiet_params(**overrides) -> _capi.PicQuiet:
+    """The reference's quiet-start parameters (``pic_quiet_defaults``) with overrides."""
+    q = _capi.PicQuiet()
+    rc = _capi.load().pic_quiet_defaults(C.byref(q))
+    if rc != 0:
+        raise PicError(rc, "pic_quiet_defaults")
+    for k, v in overrides.items():
+        if not hasattr(q, k):
+            raise KeyError(k)
+        setattr(q, k, v)
+    return q
+
+
+def quiet_start(**overrides):
+    """The reference's quiet start (``pic_quiet_start``; getUniformMaxwellianParticles,
+    maxwell.cu:676-757): dict of ions / electrons / beam, each a dict of x y z
+    px py pz arrays plus q_m and m (getMassCharge).  Keyword arguments
+    override the reference's parameters (n_ions, lx, beam_ly, ...)."""
+    q = quiet_params(**overrides)
+    n = int(q.n_ions)
+    if n < 0:
+        raise PicError(-1, "pic_quiet_start: n_ions < 0")
+    sizes = (n, 2 * n, n)
+    arrs = [[np.zeros(sz) for _ in range(6)] for sz in sizes]
+    ptrs = [(C.c_void_p * 6)(*[a.ctypes.data if a.size else None for a in group]) for group in arrs]
+    nb = C.c_int64(0)
+    q_m, m = np.zeros(3), np.zeros(3)
+    rc = _capi.load().pic_quiet_start(C.byref(q), *ptrs, C.byref(nb), dptr(q_m), dptr(m))
+    if rc != 0:
+        raise PicError(rc, "pic_quiet_start")
+    out = {}
+    for s, (name, group) in enumerate(zip(QUIET_SORTS, arrs)):
+        keep = int(nb.value) if name == "beam" else group[0].size
+        out[name] = {k: a[:keep] for k, a in zip(_PKEYS, group)}
+        out[name].update(q_m=float(q_m[s]), m=float(m[s]))
+    return out
+
+
 class Plasma:
     """Mirror of the reference's ``class Plasma`` (gpu_plasma.h:97).
 
@@ -443,25 +517,37 @@ class Plasma:
     in main.cu:14).  ``Initialize`` loads the beam-plasma species of the
     benchmark configurations (ions of q/m = ion_q_m and density 1.01*ni,
     electrons of density ni, beam of density 0.01*ni) with ``n_per_cell``
-    particles per cell per species from a seeded generator, replacing the
-    reference's hard-coded loader (maxwell.cu:676-757).
+    particles per cell per species from a seeded generator; with
+    ``loader="quiet_start"`` it loads the reference's own initial state
+    instead (InitializeCPU, init.cu:111-139: getUniformMaxwellianParticles,
+    maxwell.cu:676-757, whose parameters -- 1.6M ions, lp = 1000, the box of
+    main.cu:14 -- are its own, overridable through ``quiet``), with the charge
+    weights of getMassCharge (maxwell.cu:598-612).
     """
 
     TOTAL_STEPS = 5  # run_control.h:10
 
     def __init__(self, Nx, Ny, Nz, Lx, Ly, Lz, ni, n_per_cell, ion_q_m, tau, precision="fp64",
-                 ghosts="reference", device=0, seed=0, species=None):
+                 ghosts="reference", device=0, seed=0, species=None, loader="generator", quiet=None):
         self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
         self.Lx, self.Ly, self.Lz = Lx, Ly, Lz
         self.ni, self.n_per_cell, self.ion_q_m, self.tau = ni, n_per_cell, ion_q_m, tau
         self.seed = seed
-        if species is None:
-            species = [dict(s) for s in SPECIES_BEAM_PLASMA]
-            species[0]["q_m"] = ion_q_m
-            for s in species:
-                s["density"] = s["density"] * ni
-        self.species = species
-        table = [(s["q_m"], charge_weight(s["q_m"], s["density"], n_per_cell), s["sort"]) for s in species]
+        if loader not in ("generator", "quiet_start"):
+            raise ValueError(loader)
+        self.loader, self.quiet = loader, dict(quiet or {})
+        if loader == "quiet_start":
+            w = quiet_start(**dict(self.quiet, n_ions=0))
+            table = [(w[k]["q_m"], w[k]["m"], sort) for sort, k in enumerate(QUIET_SORTS)]
+            self.species = [dict(name=k, sort=sort, q_m=w[k]["q_m"], m=w[k]["m"]) for sort, k in enumerate(QUIET_SORTS)]
+        else:
+            if species is None:
+                species = [dict(s) for s in SPECIES_BEAM_PLASMA]
+                species[0]["q_m"] = ion_q_m
+                for s in species:
+                    s["density"] = s["density"] * ni
+            self.species = species
+            table = [(s["q_m"], charge_weight(s["q_m"], s["density"], n_per_cell), s["sort"]) for s in species]
         self.sim = PicSimulation((Nx, Ny, Nz), (Lx, Ly, Lz), tau, table, precision=precision, ghosts=ghosts,
                                  device=device)
         self.energy_history = []
@@ -469,6 +555,11 @@ class Plasma:
 
     # Initialize, init.cu:141-152
     def Initialize(self, host_generator: bool = False):
+        if self.loader == "quiet_start":
+            parts = quiet_start(**self.quiet)
+            for i, k in enumerate(QUIET_SORTS):
+                self.sim.load_particles(i, *[parts[k][a] for a in _PKEYS])
+            return
         for i, s in enumerate(self.species):
             if host_generator:
                 arrs = host_species((self.Nx, self.Ny, self.Nz), (self.Lx, self.Ly, self.Lz), i, self.n_per_cell,

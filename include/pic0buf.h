@@ -350,6 +350,51 @@ int pic_mumu_read(const char *path, pic_mumu *d);
 int pic_dump_write(pic_handle *h, const char *path);
 int pic_dump_read(pic_handle *h, const char *path);
 
+/* The reference's random numbers (rnd_uniform / rnd_gaussian, maxwell.h:17-19;
+ * g05cae / g05dde, maxwell.cu:77-170): a three-stream combined multiplicative
+ * uniform generator in Wichmann-Hill form (moduli 30269 30307 30323) and
+ * Brent's table-driven Gaussian (CACM algorithm 488).  The reference keeps the
+ * state in globals; here it is the caller's.  pic_rnd_init sets the
+ * reference's initial state (seeds 1 255 25555, stored uniform 1). */
+typedef struct pic_rnd {
+    int32_t ix, iy, iz;
+    double store;
+} pic_rnd;
+void pic_rnd_init(pic_rnd *r);
+double pic_rnd_uniform(pic_rnd *r);
+double pic_rnd_gaussian(pic_rnd *r, double mean, double sd);
+/* Brent's interval table, d[i] ~ Phi^-1(1 - 2^-(i+1)) for i = 0..40, as the
+ * reference states it (41 doubles) */
+int pic_rnd_table(double *out41);
+
+/* The reference's quiet start (getUniformMaxwellianParticles,
+ * maxwell.cu:676-757; InitUniformMaxwellianParticles, maxwell.cu:379-536),
+ * the initial state of its default run (InitializeCPU, init.cu:111-139):
+ * n_ions ions uniform in the box at rest, one beam electron on each ion inside
+ * the beam region (drift rimp along x, spread Tb*rimp) and two plasma
+ * electrons on every ion (spreads tex0 tey0 tez0, carrying the return
+ * current rbd * beam velocity inside the beam's x/y region).  Host only. */
+typedef struct pic_quiet {
+    int64_t n_ions;                     /* jmb; 1,600,000 in the reference */
+    double tex0, tey0, tez0;            /* electron thermal spreads */
+    double Tb, rimp, rbd, ni;           /* beam spread / drift / density, plasma density */
+    int meh, lp, beamf;                 /* y offset in boxes, particles per cell, return current on */
+    double lx, ly, lz;                  /* box */
+    double beam_lx, beam_ly, beam_lz;   /* beam region (centred in y and z) */
+} pic_quiet;
+/* the reference's values (maxwell.cu:680-696, 716-718) */
+int pic_quiet_defaults(pic_quiet *q);
+/* ion[6] (x y z px py pz) hold n_ions each, el[6] 2*n_ions, beam[6] n_ions;
+ * *n_beam receives the beam electrons written (beam entries past it are
+ * untouched: the reference hands n_ions beam entries to its cells whatever
+ * the count, from unset memory past it, and its electron pair j reads beam j,
+ * taken here as zero past the count -- at the reference's values the beam
+ * region is the whole box and the count is n_ions).  q_m3 / m3 (may be NULL)
+ * receive q/m and the charge weight of ions, electrons, beam (getMassCharge,
+ * maxwell.cu:598-612).  With n_ions = 0 only q_m3 and m3 are written. */
+int pic_quiet_start(const pic_quiet *q, double *const ion[6], double *const el[6], double *const beam[6],
+                    int64_t *n_beam, double *q_m3, double *m3);
+
 /* Status and errors. */
 int pic_sync(pic_handle *h);
 int pic_last_status(pic_handle *h);

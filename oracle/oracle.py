@@ -315,3 +315,73 @@ def ref_read_mumu(workdir, nt, cells):
         n = lib.ref_mumu_particles(s, a.ctypes.data_as(D))
         out.append(a[:n])
     return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's quiet start and random numbers (replay library only): the
+# generator state lives in maxwell.cu's globals, which ref_rnd_* reset / set.
+
+def _ref_rnd_lib():
+    lib = RefSim.lib()
+    lib.ref_rnd_set.argtypes = [C.c_long] * 3 + [C.c_double]
+    lib.ref_rnd_set.restype = None
+    lib.ref_rnd_reset.restype = None
+    lib.ref_rnd_uniforms.argtypes = [C.c_long, D]
+    lib.ref_rnd_uniforms.restype = None
+    lib.ref_rnd_gaussians.argtypes = [C.c_long, C.c_double, C.c_double, D]
+    lib.ref_rnd_gaussians.restype = None
+    lib.ref_quiet_init.argtypes = [C.c_int, C.c_int, D, C.c_int, D, D, D]
+    lib.ref_quiet_init.restype = C.c_long
+    lib.ref_quiet_default.argtypes = [C.POINTER(C.c_long)]
+    lib.ref_quiet_default.restype = C.c_int
+    lib.ref_mumu_particles.argtypes = [C.c_int, D]
+    lib.ref_mumu_particles.restype = C.c_long
+    return lib
+
+
+def ref_rnd(n, state=None, gaussian=None):
+    """n numbers of the reference's rnd_uniform (gaussian None) or
+    rnd_gaussian(mean, sd) (gaussian = (mean, sd)) from state (ix, iy, iz,
+    store), default the reference's initial state (maxwell.cu:46-52)."""
+    lib = _ref_rnd_lib()
+    if state is None:
+        lib.ref_rnd_reset()
+    else:
+        lib.ref_rnd_set(*[int(v) for v in state[:3]], float(state[3]))
+    out = np.zeros(int(n))
+    if gaussian is None:
+        lib.ref_rnd_uniforms(int(n), out.ctypes.data_as(D))
+    else:
+        lib.ref_rnd_gaussians(int(n), float(gaussian[0]), float(gaussian[1]), out.ctypes.data_as(D))
+    return out
+
+
+QUIET_PAR = ("tex0", "tey0", "tez0", "beam_lx", "beam_ly", "beam_lz", "lx", "ly", "lz", "Tb", "rimp", "rbd")
+
+
+def ref_quiet_init(jmb, beamf=1, meh=0, **par):
+    """The reference's InitUniformMaxwellianParticles (maxwell.cu:379-536)
+    from the initial generator state: (ion (6, jmb), electrons (6, 2 jmb),
+    beam (6, count)) as x y z px py pz rows."""
+    lib = _ref_rnd_lib()
+    p = np.array([float(par[k]) for k in QUIET_PAR])
+    ion, el, beam = np.zeros(6 * jmb), np.zeros(12 * jmb), np.zeros(6 * jmb)
+    nb = lib.ref_quiet_init(int(beamf), int(jmb), p.ctypes.data_as(D), int(meh), ion.ctypes.data_as(D),
+                            el.ctypes.data_as(D), beam.ctypes.data_as(D))
+    return ion.reshape(6, jmb), el.reshape(6, 2 * jmb), beam.reshape(6, jmb)[:, :nb]
+
+
+def ref_quiet_default():
+    """The reference's getUniformMaxwellianParticles (maxwell.cu:676-757):
+    [(n, 8) array of x y z pu pv pw m q_m] for ions, electrons, beam."""
+    lib = _ref_rnd_lib()
+    counts = (C.c_long * 3)()
+    rc = lib.ref_quiet_default(counts)
+    if rc != 0:
+        raise RuntimeError(f"getUniformMaxwellianParticles returned {rc}")
+    out = []
+    for s in range(3):
+        a = np.zeros((max(int(counts[s]), 1), 8))
+        n = lib.ref_mumu_particles(s, a.ctypes.data_as(D))
+        out.append(a[:n])
+    return out

@@ -352,6 +352,17 @@ double energy(RefSim &s) {  // GPU_getCellEnergy, wrap_kernel.cu:14-36 (serial o
 
 }  // namespace
 
+// The reference's random-number state lives in two globals of maxwell.cu
+// (cag05a: the three streams; cag05b: Brent's stored uniform) with the
+// layouts below; ref_rnd_* set and read it so each call starts from a known
+// state.
+struct cag05a { long e_1[3]; };
+struct cag05b { double e_1[2]; };
+extern cag05a cag05a_;
+extern cag05b cag05b_;
+double rnd_uniform(int dbg_print);                      // maxwell.cu:187-192
+double rnd_gaussian(double a, double b, int dbg_print);  // maxwell.cu:194-197
+
 extern "C" {
 
 void ref_set_threads(int n) { g_threads = n > 0 ? n : 1; }
@@ -503,9 +514,62 @@ long ref_get_particles(void *h, double *out, int *cell, int *sort, int *directio
 // kept here for ref_mumu_particles.
 static std::vector<Particle> g_mumu[3];
 
+void ref_rnd_set(long ix, long iy, long iz, double store) {
+    cag05a_.e_1[0] = ix;
+    cag05a_.e_1[1] = iy;
+    cag05a_.e_1[2] = iz;
+    cag05b_.e_1[0] = store;
+}
+
+void ref_rnd_get(long *ixyz, double *store) {
+    for (int a = 0; a < 3; a++) ixyz[a] = cag05a_.e_1[a];
+    *store = cag05b_.e_1[0];
+}
+
+void ref_rnd_reset() { ref_rnd_set(1, 255, 25555, 1.0); }  // cag05a_ / cag05b_ initial data
+
+// n uniforms, or n Gaussian deviates of the given mean and spread, from the
+// current state
+void ref_rnd_uniforms(long n, double *out) {
+    for (long j = 0; j < n; j++) out[j] = rnd_uniform(0);
+}
+
+void ref_rnd_gaussians(long n, double a, double b, double *out) {
+    for (long j = 0; j < n; j++) out[j] = rnd_gaussian(a, b, 0);
+}
+
+// InitUniformMaxwellianParticles (maxwell.cu:379-536) from the generator's
+// initial state.  par: tex0 tey0 tez0 beam_lx beam_ly beam_lz lx ly lz Tb rimp
+// rbd.  Outputs planar: ion[a*jmb + j], el[a*2*jmb + j], beam[a*jmb + j] for
+// a = x y z px py pz.  The beam arrays are zeroed first (the reference's are
+// unset past the beam count and its electron loop reads them there).
+// Returns the beam count.
+long ref_quiet_init(int beamf, int jmb, const double *par, int meh, double *ion, double *el, double *beam) {
+    ref_rnd_reset();
+    memset(beam, 0, sizeof(double) * 6 * (size_t)jmb);
+    int real = 0;
+    InitUniformMaxwellianParticles(beamf, jmb, par[0], par[1], par[2], par[3], par[4], par[5], &real, par[6],
+                                   par[7], par[8], meh, par[9], par[10], par[11], ion, ion + jmb, ion + 2 * jmb,
+                                   ion + 3 * jmb, ion + 4 * jmb, ion + 5 * jmb, beam, beam + jmb, beam + 2 * jmb,
+                                   beam + 3 * jmb, beam + 4 * jmb, beam + 5 * jmb, el, el + 2 * jmb,
+                                   el + 4 * jmb, el + 6 * jmb, el + 8 * jmb, el + 10 * jmb);
+    return real;
+}
+
 int ref_mumu_load(int nt, int nx, int ny, int nz, long *counts3) {
     for (auto &v : g_mumu) v.clear();
     int rc = LoadParticleData(nt, g_mumu[0], g_mumu[1], g_mumu[2], nx, ny, nz);
+    for (int s = 0; s < 3; s++) counts3[s] = (long)g_mumu[s].size();
+    return rc;
+}
+
+// The reference's quiet start, getUniformMaxwellianParticles
+// (maxwell.cu:676-757), from the generator's initial state, into the same
+// three lists (ions, electrons, beam) for ref_mumu_particles.
+int ref_quiet_default(long *counts3) {
+    ref_rnd_reset();
+    for (auto &v : g_mumu) v.clear();
+    int rc = getUniformMaxwellianParticles(g_mumu[0], g_mumu[1], g_mumu[2]);
     for (int s = 0; s < 3; s++) counts3[s] = (long)g_mumu[s].size();
     return rc;
 }

@@ -4,10 +4,13 @@ oracle/build_ref.sh and replayed by oracle/ref_driver.cu).
 
 Run in a container that has the reference sources:
     python tests/golden/make_golden.py
-Writes tests/golden/ref_small.npz and tests/golden/ref_c0.npz.  The inputs come
-from the product's host generator (pic_init_species_host, seeded); they are
+Writes tests/golden/ref_small.npz and tests/golden/ref_c0.npz, whose inputs
+come from the product's host generator (pic_init_species_host, seeded) and are
 stored in the fixture (small case) or pinned by a digest (c0 case) so the
-fixtures stand alone.
+fixtures stand alone; and tests/golden/ref_quiet.npz, the reference's own
+default run (main.cu:14: 100x4x4 cells, box 1.1424 x 0.05 x 0.05, tau 0.001)
+from the reference's own initial state (getUniformMaxwellianParticles,
+maxwell.cu:676-757, pinned by a digest).
 """
 from __future__ import annotations
 
@@ -109,10 +112,47 @@ def make_c0(steps=10):
     np.savez_compressed(os.path.join(OUT, "ref_c0.npz"), **rec)
 
 
+QUIET_SAMPLE = 4999  # every 4999th row of the canonical particle table
+
+
+def make_quiet(steps=10):
+    import oracle
+    cells, lengths, tau = (100, 4, 4), (1.1424, 0.05, 0.05), 0.001
+    sorts = oracle.ref_quiet_default()
+    sim = RefSim(cells, lengths, tau, threads=os.cpu_count() or 1)
+    rec = dict(cells=np.array(cells), lengths=np.array(lengths), tau=tau, steps=steps, sample=QUIET_SAMPLE)
+    rec["inputs_digest"] = digest(np.concatenate([P[:, a] for P in sorts for a in range(6)]))
+    for s, P in enumerate(sorts):
+        rec[f"in_s{s}_count"] = P.shape[0]
+        rec[f"in_s{s}_m"], rec[f"in_s{s}_q_m"] = P[0, 6], P[0, 7]
+        sim.add_particles(s, *[np.ascontiguousarray(P[:, a]) for a in range(6)], P[0, 6], P[0, 7])
+    for st in range(1, steps + 1):
+        assert sim.step() == 0
+        rec[f"step{st}_counts"] = sim.cell_counts()
+        rec[f"step{st}_energy"] = sim.energy_reference()
+        if st in (1, steps):
+            for f in FIELDS:
+                rec[f"step{st}_{f}"] = sim.get_field(f)
+    tab = particle_table(sim.particles())
+    tab = tab[np.lexsort((tab[:, 4], tab[:, 3], tab[:, 2], tab[:, 1], tab[:, 0]))]
+    rec["final_rows"] = tab.shape[0]
+    rec["final_particles_sample"] = tab[::QUIET_SAMPLE]
+    np.savez_compressed(os.path.join(OUT, "ref_quiet.npz"), **rec)
+
+
 if __name__ == "__main__":
     if not RefSim.available():
         sys.exit("oracle/_ref/libref0buf.so missing: run oracle/build_ref.sh where the reference sources exist")
-    make_small()
-    make_c0()
-    for f in ("ref_small.npz", "ref_c0.npz"):
+    which = sys.argv[1:] or ["small", "c0", "quiet"]
+    made = []
+    if "small" in which:
+        make_small()
+        made.append("ref_small.npz")
+    if "c0" in which:
+        make_c0()
+        made.append("ref_c0.npz")
+    if "quiet" in which:
+        make_quiet()
+        made.append("ref_quiet.npz")
+    for f in made:
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")

@@ -1,0 +1,83 @@
+"""The reference's own default run on the GPU: ``Plasma(100, 4, 4, 1.1424,
+0.05, 0.05, 1.0, 2000, 1.0, 0.001)`` (main.cu:14) from the reference's quiet
+start (InitializeCPU, init.cu:111-139: 1.6M ions, 3.2M electrons, 1.6M beam
+electrons, about 4000 particles per cell), through the reference-facing
+``Plasma`` mirror, against the fixture the reference's own functions made
+(tests/golden/ref_quiet.npz, make_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz"]
+REL = 1e-12   # plain form: relative L2 per field, relative energy
+ABS_X = 1e-12
+MAIN_CU = (100, 4, 4, 1.1424, 0.05, 0.05, 1.0, 2000, 1.0, 0.001)
+
+
+def rel_l2(a, b):
+    d = np.linalg.norm(a - b)
+    return 0.0 if d == 0.0 else d / max(np.linalg.norm(b), 1e-300)
+
+
+def fixture():
+    return np.load(os.path.join(GOLDEN, "ref_quiet.npz"))
+
+
+def canon_table(sim):
+    rows = []
+    for s in range(sim.nspecies):
+        p = sim.particles(s)
+        rows.append(np.stack([p["cell"].astype(float), np.full(p["x"].size, float(s)), p["x"], p["y"], p["z"],
+                              p["px"], p["py"], p["pz"]], 1))
+    t = np.concatenate(rows)
+    return t[np.lexsort((t[:, 4], t[:, 3], t[:, 2], t[:, 1], t[:, 0]))]
+
+
+def test_default_run_matches_reference(pkg):
+    d = fixture()
+    steps = int(d["steps"])
+    pl = pkg.Plasma(*MAIN_CU, loader="quiet_start")
+    with pl.sim as sim:
+        pl.Initialize()
+        assert [sim.num_particles(s) for s in range(3)] == [int(d[f"in_s{s}_count"]) for s in range(3)]
+        for s in range(3):
+            assert sim.cfg.species[s].m == float(d[f"in_s{s}_m"])
+            assert sim.cfg.species[s].q_m == float(d[f"in_s{s}_q_m"])
+        for nt in range(1, steps + 1):
+            pl.Step(nt)
+            assert np.array_equal(sim.cell_counts(), d[f"step{nt}_counts"]), nt
+            e_ref = float(d[f"step{nt}_energy"])
+            assert pl.energy_history[-1][1] == pytest.approx(e_ref, rel=REL), nt
+            if nt in (1, steps):
+                for f in FIELDS:
+                    assert rel_l2(sim.get_field(f), d[f"step{nt}_{f}"]) <= REL, (nt, f)
+        tab = canon_table(sim)
+        assert tab.shape[0] == int(d["final_rows"])
+        sample = tab[::int(d["sample"])]
+        ref = d["final_particles_sample"]
+        assert np.array_equal(sample[:, :2], ref[:, :2])
+        np.testing.assert_allclose(sample[:, 2:], ref[:, 2:], rtol=0, atol=ABS_X)
+
+
+def test_default_run_mixed_form(pkg):
+    """The FP32 mixed form on the same run: no particle lost, Gauss's law kept
+    to FP32 level, and the fields close to the reference's after 10 steps."""
+    d = fixture()
+    steps = int(d["steps"])
+    pl = pkg.Plasma(*MAIN_CU, loader="quiet_start", precision="fp32")
+    with pl.sim as sim:
+        pl.Initialize()
+        sim.gauss_check(set_baseline=True)
+        for nt in range(1, steps + 1):
+            pl.Step(nt)
+        assert sim.num_particles() == int(d["final_rows"])
+        g = sim.gauss_check()
+        assert g[0] < 2e-5 * g[1], g
+        errs = {f: rel_l2(sim.get_field(f), d[f"step{steps}_{f}"]) for f in FIELDS}
+        assert max(errs.values()) < 1e-3, errs
+        assert pl.energy_history[-1][1] == pytest.approx(float(d[f"step{steps}_energy"]), rel=1e-3)

@@ -1,0 +1,165 @@
+"""The reference's quiet start on the host (pic_rnd_*, pic_quiet_start):
+the random numbers and the initial particles against the reference's own
+rnd_uniform / rnd_gaussian / InitUniformMaxwellianParticles /
+getUniformMaxwellianParticles (maxwell.cu:77-197, 379-536, 676-757) from the
+replay library, bit for bit, and the statistics the initialiser promises."""
+import hashlib
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+KEYS = ("x", "y", "z", "px", "py", "pz")
+needs_ref = pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref0buf.so")),
+                               reason="needs the reference replay library (oracle/build_ref.sh)")
+
+PAR = dict(tex0=1e-3, tey0=2e-3, tez0=3e-3, beam_lx=1.1424, beam_ly=0.05, beam_lz=0.05, lx=1.1424, ly=0.05,
+           lz=0.05, Tb=0.14, rimp=0.2, rbd=2e-3)
+
+
+def upper_quantile(p):
+    """x with 1 - Phi(x) = p (bisection on erfc; p >= 2^-41)."""
+    lo, hi = 0.0, 10.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if 0.5 * math.erfc(mid / math.sqrt(2.0)) > p:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def test_table_is_the_normal_quantiles(pkg):
+    """Brent's table holds Phi^-1(1 - 2^-(i+1)) to 15 decimals."""
+    d = pkg.Rnd.table()
+    assert d[0] == 0.0 and np.all(np.diff(d) > 0)
+    for i in range(1, 41):
+        assert abs(d[i] - upper_quantile(2.0 ** -(i + 1))) < 2e-15, i
+
+
+def test_uniform_stream_properties(pkg):
+    r = pkg.Rnd()
+    u = r.uniform(200000)
+    assert np.all((u >= 0) & (u < 1))
+    assert abs(u.mean() - 0.5) < 3e-3 and abs(u.var() - 1 / 12) < 2e-3
+    # the state is the caller's: two generators from the same state agree
+    a, b = pkg.Rnd(5, 6, 7, 0.3), pkg.Rnd(5, 6, 7, 0.3)
+    assert np.array_equal(a.gaussian(0.0, 1.0, 100), b.gaussian(0.0, 1.0, 100))
+
+
+def test_gaussian_moments(pkg):
+    g = pkg.Rnd().gaussian(0.5, 2.0, 200000)
+    assert abs(g.mean() - 0.5) < 0.03 and abs(g.std() - 2.0) < 0.02
+    z = (g - 0.5) / 2.0
+    assert abs(np.mean(z ** 4) - 3.0) < 0.1          # normal kurtosis
+    assert abs(np.mean(np.abs(z) > 3.0) - 2.7e-3) < 6e-4
+
+
+@needs_ref
+def test_uniform_matches_reference(pkg, oracle_mod):
+    r = pkg.Rnd()
+    assert np.array_equal(r.uniform(100000), oracle_mod.ref_rnd(100000))
+    s = (30000, 17, 30322, 1.0)
+    assert np.array_equal(pkg.Rnd(*s).uniform(1000), oracle_mod.ref_rnd(1000, s))
+
+
+@needs_ref
+@pytest.mark.parametrize("k", range(0, 46))
+def test_gaussian_matches_reference_in_every_interval(pkg, oracle_mod, k):
+    """A stored uniform of 0.75 * 2^-k starts the deviate in table interval
+    k + 1 (capped at 40), so k = 0..45 reaches every entry of the table."""
+    state = (1234 + k, 777 + 3 * k, 9 + k, 0.75 * 2.0 ** -k)
+    mine = pkg.Rnd(*state).gaussian(0.3, 1.7, 60)
+    assert np.array_equal(mine, oracle_mod.ref_rnd(60, state, gaussian=(0.3, 1.7)))
+
+
+@needs_ref
+@pytest.mark.parametrize("case", [
+    dict(n_ions=4000, meh=0, beamf=1),
+    dict(n_ions=4000, meh=0, beamf=0),
+    dict(n_ions=3000, meh=0, beamf=1, beam_lx=0.6, beam_ly=0.03, beam_lz=0.02),
+    dict(n_ions=3000, meh=1, beamf=1, beam_lx=0.6, beam_ly=0.03),
+    dict(n_ions=1, meh=0, beamf=1),
+])
+def test_quiet_start_matches_reference(pkg, oracle_mod, case):
+    """InitUniformMaxwellianParticles on the same parameters, including a
+    beam region smaller than the box (electron pairs past the beam count read
+    beam entries the reference leaves unset; both read zero here) and a box
+    shifted by meh that holds no beam."""
+    par = dict(PAR, **{k: v for k, v in case.items() if k in PAR})
+    ion, el, beam = oracle_mod.ref_quiet_init(case["n_ions"], beamf=case["beamf"], meh=case["meh"], **par)
+    got = pkg.quiet_start(n_ions=case["n_ions"], meh=case["meh"], beamf=case["beamf"], **par)
+    for name, ref in (("ions", ion), ("electrons", el), ("beam", beam)):
+        assert got[name]["x"].size == ref.shape[1], name
+        for a, k in enumerate(KEYS):
+            assert np.array_equal(got[name][k], ref[a]), (name, k)
+
+
+@needs_ref
+def test_default_quiet_start_matches_reference(pkg, oracle_mod):
+    """The reference's default initial state: 1.6M ions, 3.2M electrons and
+    1.6M beam electrons, every value and the charge weights identical."""
+    ref = oracle_mod.ref_quiet_default()
+    got = pkg.quiet_start()
+    for s, name in enumerate(pkg.plasma.QUIET_SORTS):
+        r = ref[s]
+        assert got[name]["x"].size == r.shape[0], name
+        for a, k in enumerate(KEYS):
+            assert np.array_equal(got[name][k], r[:, a]), (name, k)
+        assert np.all(r[:, 6] == got[name]["m"]) and np.all(r[:, 7] == got[name]["q_m"])
+
+
+def test_default_quiet_start_matches_fixture_digest(pkg):
+    """The same pin without the replay library: the digest of the reference's
+    own default initial state stored in tests/golden/ref_quiet.npz."""
+    d = np.load(os.path.join(GOLDEN, "ref_quiet.npz"))
+    got = pkg.quiet_start()
+    a = np.concatenate([got[name][k] for name in pkg.plasma.QUIET_SORTS for k in KEYS])
+    a = np.where(a == 0.0, 0.0, a)
+    assert hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest() == str(d["inputs_digest"])
+    for s, name in enumerate(pkg.plasma.QUIET_SORTS):
+        assert got[name]["x"].size == int(d[f"in_s{s}_count"])
+        assert got[name]["m"] == float(d[f"in_s{s}_m"]) and got[name]["q_m"] == float(d[f"in_s{s}_q_m"])
+
+
+def test_quiet_start_physics(pkg):
+    """What the initialiser promises: ions uniform at rest; electron pairs on
+    their ion with opposite transverse momenta; the beam drifting at rimp with
+    spread Tb*rimp; the plasma electrons' mean current cancelling the beam's
+    (charge weights from getMassCharge)."""
+    q = pkg.quiet_params()
+    n = 200000
+    st = pkg.quiet_start(n_ions=n)
+    ion, el, beam = st["ions"], st["electrons"], st["beam"]
+    assert beam["x"].size == n                      # the beam region is the box
+    assert np.all(ion["px"] == 0) and np.all(ion["py"] == 0) and np.all(ion["pz"] == 0)
+    for k, L in (("x", q.lx), ("y", q.ly), ("z", q.lz)):
+        assert ion[k].min() >= 0 and ion[k].max() < L
+        assert abs(ion[k].mean() / L - 0.5) < 5e-3
+        assert np.array_equal(el[k][0::2], ion[k]) and np.array_equal(el[k][1::2], ion[k])
+    assert np.array_equal(np.sign(el["py"][0::2]), -np.sign(el["py"][1::2]))
+    gb = np.sqrt(1 + beam["px"] ** 2 + beam["py"] ** 2 + beam["pz"] ** 2)
+    vx = beam["px"] / gb
+    assert abs(vx.mean() - q.rimp) < 1e-3 and abs(vx.std() - q.Tb * q.rimp) < 1e-3
+    ge = np.sqrt(1 + el["px"] ** 2 + el["py"] ** 2 + el["pz"] ** 2)
+    j_el = st["electrons"]["m"] * np.sum(el["px"] / ge)
+    j_beam = st["beam"]["m"] * np.sum(vx)
+    assert abs(j_el + j_beam) < 1e-3 * abs(j_beam)  # return current
+    assert st["ions"]["q_m"] == 1 / 1836 and st["electrons"]["q_m"] == -1 and st["beam"]["q_m"] == -1
+    assert st["ions"]["m"] == (q.ni + q.rbd) / q.lp and st["electrons"]["m"] == -q.ni / q.lp / 2
+    assert st["beam"]["m"] == -q.rbd / q.lp
+    # neutral: ion charge = electron + beam charge
+    assert abs(n * st["ions"]["m"] + 2 * n * st["electrons"]["m"] + n * st["beam"]["m"]) < 1e-12 * n * st["ions"]["m"]
+
+
+def test_quiet_start_arguments(pkg):
+    with pytest.raises(pkg.PicError):
+        pkg.quiet_start(n_ions=10, lp=0)
+    with pytest.raises(KeyError):
+        pkg.quiet_params(nonsense=1)
+    w = pkg.quiet_start(n_ions=0)
+    q = pkg.quiet_params()
+    assert all(w[s]["x"].size == 0 for s in w) and w["beam"]["m"] == -q.rbd / q.lp
