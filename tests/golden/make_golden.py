@@ -112,6 +112,17 @@ def make_c0(steps=10):
     np.savez_compressed(os.path.join(OUT, "ref_c0.npz"), **rec)
 
 
+def control_points_dat(path):
+    """nt, num and the twelve RMS differences of the reference's
+    control_points.dat line (names Ex .. Qz), plus its particle figure."""
+    words = open(path).read().split()
+    rec = {"cp_nt": int(words[words.index("nt") + 1]), "cp_num": int(words[words.index("num") + 1])}
+    names = [n for n in FIELDS] + ["particles"]
+    rec["cp_names"] = np.array(names)
+    rec["cp_rms"] = np.array([float(words[words.index(n) + 1]) for n in names])
+    return rec
+
+
 QUIET_SAMPLE = 4999  # every 4999th row of the canonical particle table
 
 
@@ -130,9 +141,13 @@ def make_quiet(steps=10):
         assert sim.step() == 0
         rec[f"step{st}_counts"] = sim.cell_counts()
         rec[f"step{st}_energy"] = sim.energy_reference()
-        if st in (1, steps):
+        if st in (1, 5, steps):
             for f in FIELDS:
                 rec[f"step{st}_{f}"] = sim.get_field(f)
+    # the reference's own record of its GPU run of this case against its
+    # Fortran original (control_points.dat, written by checkControlPoint,
+    # gpu_plasma.h:1170-1284): RMS differences at step 5, control point 600
+    rec.update(control_points_dat(os.path.join(os.environ.get("REF_DIR", "/root/reference"), "control_points.dat")))
     tab = particle_table(sim.particles())
     tab = tab[np.lexsort((tab[:, 4], tab[:, 3], tab[:, 2], tab[:, 1], tab[:, 0]))]
     rec["final_rows"] = tab.shape[0]
