@@ -38,6 +38,16 @@ int cuda_err(pic_handle *h, cudaError_t e, const char *where) {
     return set_err(h, (int)e, buf);
 }
 
+cudaError_t dev_alloc(pic_handle *h, void **p, size_t bytes) {
+    (void)h;
+    return cudaMalloc(p, bytes > 0 ? bytes : 16);
+}
+
+void dev_free(pic_handle *h, void *p) {
+    (void)h;
+    if (p) cudaFree(p);
+}
+
 
 size_t elem_particle(int mixed) { return mixed ? 28 : 52; }
 
@@ -61,9 +71,9 @@ StepParams make_params(pic_handle *h) {
 
 void free_alt(pic_handle *h, int s) {
     auto &S = h->sp[s];
-    if (S.alt_cell) cudaFree(S.alt_cell);
+    dev_free(h, S.alt_cell);
     for (float *&a : S.alt) {
-        if (a) cudaFree(a);
+        dev_free(h, a);
         a = nullptr;
     }
     S.alt_cell = nullptr;
@@ -74,8 +84,7 @@ void free_species(pic_handle *h, int s) {
     SpeciesView &v = h->sp[s].v;
     void *ptrs[] = {v.x, v.y, v.z, v.px, v.py, v.pz, v.ox, v.oy, v.oz, v.fx, v.fy, v.fz, v.cell, v.tile_start,
                     v.tile_count};
-    for (void *p : ptrs)
-        if (p) cudaFree(p);
+    for (void *p : ptrs) dev_free(h, p);
     double q_m = v.q_m, m = v.m;
     memset(&v, 0, sizeof(v));
     v.q_m = q_m;
@@ -108,20 +117,20 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
     free_species(h, s);
     SpeciesView &v = h->sp[s].v;
     size_t n = (size_t)acc;
-    CK(cudaMalloc(&v.cell, n * sizeof(int)), "alloc cell");
+    CK(dev_alloc_n(h, &v.cell, n), "alloc cell");
     if (!h->mixed) {
         double **arr[6] = {&v.x, &v.y, &v.z, &v.px, &v.py, &v.pz};
-        for (auto a : arr) CK(cudaMalloc(a, n * sizeof(double)), "alloc particles");
+        for (auto a : arr) CK(dev_alloc_n(h, a, n), "alloc particles");
     } else {
         float **arr[6] = {&v.ox, &v.oy, &v.oz, &v.fx, &v.fy, &v.fz};
-        for (auto a : arr) CK(cudaMalloc(a, n * sizeof(float)), "alloc particles");
+        for (auto a : arr) CK(dev_alloc_n(h, a, n), "alloc particles");
         // second set for the per-tile cell sort (maybe_sort), allocated with the bins
         auto &S = h->sp[s];
-        CK(cudaMalloc(&S.alt_cell, n * sizeof(int)), "alloc sort buffer");
-        for (float *&a : S.alt) CK(cudaMalloc(&a, n * sizeof(float)), "alloc sort buffer");
+        CK(dev_alloc_n(h, &S.alt_cell, n), "alloc sort buffer");
+        for (float *&a : S.alt) CK(dev_alloc_n(h, &a, n), "alloc sort buffer");
     }
-    CK(cudaMalloc(&v.tile_start, (g.ntiles + 1) * sizeof(int)), "alloc tile_start");
-    CK(cudaMalloc(&v.tile_count, g.ntiles * sizeof(int)), "alloc tile_count");
+    CK(dev_alloc_n(h, &v.tile_start, (size_t)g.ntiles + 1), "alloc tile_start");
+    CK(dev_alloc_n(h, &v.tile_count, (size_t)g.ntiles), "alloc tile_count");
     CK(cudaMemcpyAsync(v.tile_start, start.data(), (g.ntiles + 1) * sizeof(int), cudaMemcpyHostToDevice, h->stream),
        "upload tile_start");
     CK(cudaMemsetAsync(v.cell, 0xff, n * sizeof(int), h->stream), "clear cells");
@@ -152,20 +161,20 @@ using ScatterFn = std::function<cudaError_t(const SpeciesView &, int *)>;
 int build_bins_with(pic_handle *h, int s, int64_t n, int *cell, const ScatterFn &scatter, int64_t *inserted) {
     const Grid &g = h->g;
     int *tc = nullptr;
-    CK(cudaMalloc(&tc, g.ntiles * sizeof(int)), "alloc tile counts");
+    CK(dev_alloc_n(h, &tc, (size_t)g.ntiles), "alloc tile counts");
     CK(cudaMemsetAsync(tc, 0, g.ntiles * sizeof(int), h->stream), "memset");
     CK(tile_histogram(g, n, cell, tc, h->stream), "tile histogram");
     std::vector<int> counts(g.ntiles);
     CK(cudaMemcpyAsync(counts.data(), tc, g.ntiles * sizeof(int), cudaMemcpyDeviceToHost, h->stream), "counts");
     CK(cudaStreamSynchronize(h->stream), "sync");
     int rc = alloc_species(h, s, counts);
-    if (rc) { cudaFree(tc); return rc; }
+    if (rc) { dev_free(h, tc); return rc; }
     CK(cudaMemsetAsync(tc, 0, g.ntiles * sizeof(int), h->stream), "memset");
     CK(scatter(h->sp[s].v, tc), "scatter");
     CK(cudaMemcpyAsync(h->sp[s].v.tile_count, tc, g.ntiles * sizeof(int), cudaMemcpyDeviceToDevice, h->stream),
        "tile counts");
+    dev_free(h, tc);
     CK(cudaStreamSynchronize(h->stream), "sync");
-    cudaFree(tc);
     int64_t tot = 0;
     for (int c : counts) tot += c;
     if (inserted) *inserted = tot;
@@ -205,10 +214,10 @@ int tile_counts(pic_handle *h, int s, std::vector<int> &counts) {
 int load_device(pic_handle *h, int s, int64_t n, const double *x, const double *y, const double *z,
                 const double *px, const double *py, const double *pz, int64_t *inserted) {
     int *cell = nullptr;
-    CK(cudaMalloc(&cell, (size_t)(n > 0 ? n : 1) * sizeof(int)), "alloc cell");
+    CK(dev_alloc_n(h, &cell, (size_t)(n > 0 ? n : 1)), "alloc cell");
     CK(place_particles_plain(h->g, n, x, y, z, cell, h->stream), "place");
     int rc = build_bins(h, s, n, cell, x, y, z, px, py, pz, inserted);
-    cudaFree(cell);
+    dev_free(h, cell);
     return rc;
 }
 
@@ -229,10 +238,10 @@ int rebin_species(pic_handle *h, int s, unsigned n_out) {
     int *cell = nullptr;
     int64_t *ddst = nullptr;
     unsigned *ctr = nullptr;
-    CK(cudaMalloc(&buf, (size_t)(nmax > 0 ? nmax : 1) * 6 * sizeof(double)), "rebin buffer");
-    CK(cudaMalloc(&cell, (size_t)(nmax > 0 ? nmax : 1) * sizeof(int)), "rebin cells");
-    CK(cudaMalloc(&ddst, (g.ntiles + 1) * sizeof(int64_t)), "rebin starts");
-    CK(cudaMalloc(&ctr, sizeof(unsigned)), "rebin counter");
+    CK(dev_alloc_n(h, &buf, (size_t)(nmax > 0 ? nmax : 1) * 6), "rebin buffer");
+    CK(dev_alloc_n(h, &cell, (size_t)(nmax > 0 ? nmax : 1)), "rebin cells");
+    CK(dev_alloc_n(h, &ddst, (size_t)g.ntiles + 1), "rebin starts");
+    CK(dev_alloc_n(h, &ctr, 1), "rebin counter");
     CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned), h->stream), "memset");
     CK(cudaMemcpyAsync(ddst, dstart.data(), (g.ntiles + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream),
        "starts");
@@ -245,10 +254,10 @@ int rebin_species(pic_handle *h, int s, unsigned n_out) {
     CK(cudaMemcpyAsync(&extra, ctr, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream), "counter");
     CK(cudaStreamSynchronize(h->stream), "sync");
     int rc = build_bins(h, s, acc + extra, cell, x, y, z, px, py, pz, nullptr);
-    cudaFree(buf);
-    cudaFree(cell);
-    cudaFree(ddst);
-    cudaFree(ctr);
+    dev_free(h, buf);
+    dev_free(h, cell);
+    dev_free(h, ddst);
+    dev_free(h, ctr);
     return rc;
 }
 
@@ -488,6 +497,9 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e) { delete h; return (int)e; }
     for (int i = 0; i < 6; i++) cudaEventCreate(&h->ev[i]);
+    if ((e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    for (int i = 0; i < 5; i++)
+        if ((e = cudaEventCreateWithFlags(&h->lev[i], cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     size_t nodes = g.nodes_pitched();
     for (int fi = 0; fi < PIC_FIELD_COUNT; fi++) {
         size_t es = sizeof(double);
@@ -533,6 +545,9 @@ int pic_destroy(pic_handle *h) {
         if (d) cudaFree(d);
     for (int i = 0; i < 6; i++)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    for (int i = 0; i < 5; i++)
+        if (h->lev[i]) cudaEventDestroy(h->lev[i]);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return PIC_OK;
@@ -546,12 +561,12 @@ int pic_load_particles(pic_handle *h, int species, int64_t n, const double *x, c
     if (rc) return rc;
     size_t N = (size_t)(n > 0 ? n : 1);
     double *buf = nullptr;
-    CK(cudaMalloc(&buf, N * 6 * sizeof(double)), "alloc load buffer");
+    CK(dev_alloc_n(h, &buf, N * 6), "alloc load buffer");
     const double *src[6] = {x, y, z, px, py, pz};
     for (int a = 0; a < 6; a++)
         if (n > 0) CK(cudaMemcpyAsync(buf + a * N, src[a], (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream), "H2D particles");
     rc = load_device(h, species, n, buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N, inserted);
-    cudaFree(buf);
+    dev_free(h, buf);
     return rc;
 }
 
@@ -564,6 +579,15 @@ int pic_load_particles_device(pic_handle *h, int species, int64_t n, const doubl
     return load_device(h, species, n, x, y, z, px, py, pz, inserted);
 }
 
+// Host -> device in chunks on a second stream, overlapped with the device
+// work on the handle's stream (two staging buffers per pass):
+//   pass 1  cells and offsets: each chunk is validated and placed
+//           (place_particles_cells) and counted per tile as soon as it lands;
+//   bins    allocated from the tile counts (one host sync);
+//   pass 2  momenta: each chunk is scattered into the bins as it lands.
+// Every byte crosses the bus once; the copy engine and the kernels overlap.
+static constexpr int64_t kLoadChunk = 1 << 24;  // particles per staged chunk
+
 int pic_load_particles_cells(pic_handle *h, int species, int64_t n, const int32_t *cell, const float *ox,
                              const float *oy, const float *oz, const float *px, const float *py, const float *pz,
                              int64_t *inserted) {
@@ -571,31 +595,87 @@ int pic_load_particles_cells(pic_handle *h, int species, int64_t n, const int32_
     if (n > 0 && (!cell || !ox || !oy || !oz || !px || !py || !pz)) return set_err(h, PIC_ERR_ARG, "null array");
     int rc = set_device(h);
     if (rc) return rc;
-    size_t N = (size_t)(n > 0 ? n : 1);
-    float *buf = nullptr;
-    int *rc_cell = nullptr, *icell = nullptr;
-    CK(cudaMalloc(&buf, N * 6 * sizeof(float)), "alloc load buffer");
-    CK(cudaMalloc(&rc_cell, N * sizeof(int)), "alloc load buffer");
-    CK(cudaMalloc(&icell, N * sizeof(int)), "alloc load buffer");
-    const float *src[6] = {ox, oy, oz, px, py, pz};
-    if (n > 0) {
-        for (int a = 0; a < 6; a++)
-            CK(cudaMemcpyAsync(buf + a * N, src[a], (size_t)n * sizeof(float), cudaMemcpyHostToDevice, h->stream),
-               "H2D particles");
-        CK(cudaMemcpyAsync(rc_cell, cell, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, h->stream), "H2D cells");
-    }
-    const float *fo[6] = {buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N};
-    CK(place_particles_cells(h->g, n, rc_cell, fo[0], fo[1], fo[2], icell, h->stream), "place");
     const Grid &g = h->g;
-    int mixed = h->mixed;
-    cudaStream_t st = h->stream;
-    rc = build_bins_with(h, species, n, icell, [&](const SpeciesView &v, int *fill) {
-        return scatter_to_bins_f(g, mixed, n, icell, fo[0], fo[1], fo[2], fo[3], fo[4], fo[5], v, fill, st);
-    }, inserted);
-    cudaFree(buf);
-    cudaFree(rc_cell);
-    cudaFree(icell);
-    return rc;
+    cudaStream_t st = h->stream, cs = h->copy_stream;
+    const size_t N = (size_t)(n > 0 ? n : 1);
+    const size_t C = (size_t)std::min<int64_t>(kLoadChunk, n > 0 ? n : 1);
+    const int64_t nchunks = (n + kLoadChunk - 1) / kLoadChunk;
+    int *icell = nullptr, *tc = nullptr, *stage_cell[2] = {nullptr, nullptr};
+    float *off[3] = {nullptr, nullptr, nullptr}, *stage_mom[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    auto release = [&]() {
+        dev_free(h, icell);
+        dev_free(h, tc);
+        for (int b = 0; b < 2; b++) {
+            dev_free(h, stage_cell[b]);
+            for (int a = 0; a < 3; a++) dev_free(h, stage_mom[b][a]);
+        }
+        for (int a = 0; a < 3; a++) dev_free(h, off[a]);
+    };
+    auto ck = [&](cudaError_t e, const char *where) {
+        if (e == cudaSuccess) return PIC_OK;
+        cudaStreamSynchronize(cs);
+        release();
+        return cuda_err(h, e, where);
+    };
+#define LCK(expr, where) do { int r_ = ck((expr), (where)); if (r_) return r_; } while (0)
+    LCK(dev_alloc_n(h, &icell, N), "alloc load buffer");
+    LCK(dev_alloc_n(h, &tc, (size_t)g.ntiles), "alloc tile counts");
+    for (int a = 0; a < 3; a++) LCK(dev_alloc_n(h, &off[a], N), "alloc load buffer");
+    for (int b = 0; b < 2; b++) {
+        LCK(dev_alloc_n(h, &stage_cell[b], C), "alloc load buffer");
+        for (int a = 0; a < 3; a++) LCK(dev_alloc_n(h, &stage_mom[b][a], C), "alloc load buffer");
+    }
+    LCK(cudaMemsetAsync(tc, 0, g.ntiles * sizeof(int), st), "memset");
+    // the copy stream may use the new memory once its allocation is ordered before it
+    cudaEvent_t ready = h->lev[0], landed[2] = {h->lev[1], h->lev[2]}, used[2] = {h->lev[3], h->lev[4]};
+    LCK(cudaEventRecord(ready, st), "event");
+    LCK(cudaStreamWaitEvent(cs, ready, 0), "event");
+    const float *osrc[3] = {ox, oy, oz}, *psrc[3] = {px, py, pz};
+    for (int64_t c = 0; c < nchunks; c++) {  // pass 1
+        const int b = (int)(c & 1);
+        const size_t o = (size_t)c * kLoadChunk, m = (size_t)std::min<int64_t>(kLoadChunk, n - (int64_t)o);
+        if (c >= 2) LCK(cudaStreamWaitEvent(cs, used[b], 0), "event");
+        LCK(cudaMemcpyAsync(stage_cell[b], cell + o, m * sizeof(int), cudaMemcpyHostToDevice, cs), "H2D cells");
+        for (int a = 0; a < 3; a++)
+            LCK(cudaMemcpyAsync(off[a] + o, osrc[a] + o, m * sizeof(float), cudaMemcpyHostToDevice, cs), "H2D offsets");
+        LCK(cudaEventRecord(landed[b], cs), "event");
+        LCK(cudaStreamWaitEvent(st, landed[b], 0), "event");
+        LCK(place_particles_cells(g, (int64_t)m, stage_cell[b], off[0] + o, off[1] + o, off[2] + o, icell + o, st),
+            "place");
+        LCK(tile_histogram(g, (int64_t)m, icell + o, tc, st), "tile histogram");
+        LCK(cudaEventRecord(used[b], st), "event");
+    }
+    std::vector<int> counts(g.ntiles);
+    LCK(cudaMemcpyAsync(counts.data(), tc, g.ntiles * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
+    LCK(cudaStreamSynchronize(st), "sync");
+    rc = alloc_species(h, species, counts);
+    if (rc) { release(); return rc; }
+    SpeciesView v = h->sp[species].v;
+    LCK(cudaMemsetAsync(tc, 0, g.ntiles * sizeof(int), st), "memset");
+    LCK(cudaEventRecord(ready, st), "event");
+    LCK(cudaStreamWaitEvent(cs, ready, 0), "event");
+    for (int64_t c = 0; c < nchunks; c++) {  // pass 2
+        const int b = (int)(c & 1);
+        const size_t o = (size_t)c * kLoadChunk, m = (size_t)std::min<int64_t>(kLoadChunk, n - (int64_t)o);
+        if (c >= 2) LCK(cudaStreamWaitEvent(cs, used[b], 0), "event");
+        for (int a = 0; a < 3; a++)
+            LCK(cudaMemcpyAsync(stage_mom[b][a], psrc[a] + o, m * sizeof(float), cudaMemcpyHostToDevice, cs),
+                "H2D momenta");
+        LCK(cudaEventRecord(landed[b], cs), "event");
+        LCK(cudaStreamWaitEvent(st, landed[b], 0), "event");
+        LCK(scatter_to_bins_f(g, h->mixed, (int64_t)m, icell + o, off[0] + o, off[1] + o, off[2] + o,
+                              stage_mom[b][0], stage_mom[b][1], stage_mom[b][2], v, tc, st), "scatter");
+        LCK(cudaEventRecord(used[b], st), "event");
+    }
+    LCK(cudaMemcpyAsync(v.tile_count, tc, g.ntiles * sizeof(int), cudaMemcpyDeviceToDevice, st), "tile counts");
+    release();
+    LCK(cudaStreamSynchronize(st), "sync");
+#undef LCK
+    int64_t tot = 0;
+    for (int c : counts) tot += c;
+    if (inserted) *inserted = tot;
+    h->kin_valid = 0;
+    return ensure_outbox(h);
 }
 
 int pic_get_particles_cells(pic_handle *h, int species, int64_t cap, int32_t *cell, float *ox, float *oy, float *oz,

@@ -33,14 +33,34 @@ __global__ void k_place(Grid g, int64_t n, const double *__restrict__ x, const d
     cell[p] = c;
 }
 
-__global__ void k_tile_hist(Grid g, int64_t n, const int *__restrict__ cell, int *tile_counts) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    int c = cell[p];
-    if (c < 0) return;
+// Tile of a flat list entry (-1 for a rejected entry or past the end).
+__device__ __forceinline__ int entry_tile(const Grid &g, int64_t p, int64_t n, const int *__restrict__ cell, int &c) {
+    c = p < n ? cell[p] : -1;
+    if (c < 0) return -1;
     int i, l, k;
     cell_ijk(g, c, i, l, k);
-    atomicAdd(&tile_counts[g.tile_of_cell(i, l, k)], 1);
+    return g.tile_of_cell(i, l, k);
+}
+
+// Warp-aggregated per-tile counter: the lanes of a warp with the same tile
+// (match.any) take one atomic, issued by their first lane, and each gets the
+// old count plus its rank in the group.  Lists arrive grouped by tile, so
+// per-lane atomics would put 32 lanes on one address; ranks keep the lanes'
+// order, so a warp's entries land contiguously and in input order.  All 32
+// lanes must call it.
+__device__ __forceinline__ int tile_claim(int *ctr, int t) {
+    const unsigned peers = __match_any_sync(0xffffffffu, t);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int base = 0;
+    if (t >= 0 && lane == leader) base = atomicAdd(&ctr[t], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1));
+}
+
+__global__ void k_tile_hist(Grid g, int64_t n, const int *__restrict__ cell, int *tile_counts) {
+    int c;
+    const int t = entry_tile(g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, n, cell, c);
+    tile_claim(tile_counts, t);
 }
 
 __device__ __forceinline__ float to_offset(double x, int i, double h) {
@@ -52,14 +72,14 @@ __device__ __forceinline__ float to_offset(double x, int i, double h) {
 __global__ void k_scatter(Grid g, int mixed, int64_t n, const int *__restrict__ cell, const double *__restrict__ x,
                           const double *__restrict__ y, const double *__restrict__ z, const double *__restrict__ px,
                           const double *__restrict__ py, const double *__restrict__ pz, SpeciesView S, int *fill) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    int c = cell[p];
-    if (c < 0) return;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int c;
+    const int t = entry_tile(g, p, n, cell, c);
+    const int rank = tile_claim(fill, t);
+    if (t < 0) return;
     int i, l, k;
     cell_ijk(g, c, i, l, k);
-    int t = g.tile_of_cell(i, l, k);
-    int slot = S.tile_start[t] + atomicAdd(&fill[t], 1);
+    int slot = S.tile_start[t] + rank;
     S.cell[slot] = c;
     if (!mixed) {
         S.x[slot] = x[p]; S.y[slot] = y[p]; S.z[slot] = z[p];
@@ -90,14 +110,14 @@ __global__ void k_place_cells(Grid g, int64_t n, const int *__restrict__ ref_cel
 __global__ void k_scatter_f(Grid g, int mixed, int64_t n, const int *__restrict__ cell, const float *__restrict__ ox,
                             const float *__restrict__ oy, const float *__restrict__ oz, const float *__restrict__ px,
                             const float *__restrict__ py, const float *__restrict__ pz, SpeciesView S, int *fill) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    int c = cell[p];
-    if (c < 0) return;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int c;
+    const int t = entry_tile(g, p, n, cell, c);
+    const int rank = tile_claim(fill, t);
+    if (t < 0) return;
     int i, l, k;
     cell_ijk(g, c, i, l, k);
-    int t = g.tile_of_cell(i, l, k);
-    int slot = S.tile_start[t] + atomicAdd(&fill[t], 1);
+    int slot = S.tile_start[t] + rank;
     S.cell[slot] = c;
     if (mixed) {
         S.ox[slot] = ox[p]; S.oy[slot] = oy[p]; S.oz[slot] = oz[p];

@@ -55,6 +55,11 @@ struct pic_handle {
     double *rho, *gauss, *gauss0;
     int gauss_has_base;
     int branch_record;  // the next pic_forward records its discrete choices (pic_branch_record)
+    // second stream and events of the chunked host->device load
+    // (pic_load_particles_cells): copies run there while the handle's stream
+    // places and scatters the previous chunk
+    cudaStream_t copy_stream;
+    cudaEvent_t lev[5];
 };
 
 namespace pic_host {
@@ -63,6 +68,15 @@ int set_err(pic_handle *h, int code, const char *msg);
 int cuda_err(pic_handle *h, cudaError_t e, const char *where);
 int set_device(pic_handle *h);
 int need_particles(pic_handle *h);
+// device memory of the particle bins and of load/rebin staging (cudaMalloc:
+// a stream-ordered pool was measured at 1-4 s to grow by the ~19 GB of one
+// c2 species' bins, against 0.16 s for the whole load with cudaMalloc)
+cudaError_t dev_alloc(pic_handle *h, void **p, size_t bytes);
+void dev_free(pic_handle *h, void *p);
+template <class T>
+cudaError_t dev_alloc_n(pic_handle *h, T **p, size_t n) {
+    return dev_alloc(h, (void **)p, n * sizeof(T));
+}
 // kernel parameters of the current state (species views, fields, outbox, status)
 pic::StepParams make_params(pic_handle *h);
 // flat device list of one species (packed cell, FP64 global positions and
