@@ -173,8 +173,23 @@ __device__ __forceinline__ PartM load_part(const SpeciesView &S, int slot) {
 //     tile J, so a few such lanes do not stall the other lanes of their warp.
 constexpr int kGroups = 4;
 constexpr int kSlots = 54;
-constexpr int kQueue = 64;  // queued segments per warp
-static_assert(kHoleMax * sizeof(int) <= (kPushThreads / 32) * kQueue * 2 * sizeof(float4),
+// 320 threads, two CTAs per SM (96 registers, no spills): 20 warps per SM
+// against 16 with 256 threads at 123 registers; the kernel is issue-bound and
+// the extra warps cut the c2 push from 30.5 to 29.2 ms (288 and 384 threads
+// measured slower)
+#ifndef PIC_MIXED_THREADS
+#define PIC_MIXED_THREADS 320
+#endif
+#ifndef PIC_MIXED_MIN_BLOCKS
+#define PIC_MIXED_MIN_BLOCKS 2
+#endif
+#ifndef PIC_MIXED_QUEUE
+#define PIC_MIXED_QUEUE 64
+#endif
+constexpr int kMixedThreads = PIC_MIXED_THREADS;  // threads per CTA of k_push_mixed
+constexpr int kQueue = PIC_MIXED_QUEUE;           // queued segments per warp
+static_assert(kMixedThreads % 32 == 0, "whole warps");
+static_assert(kHoleMax * sizeof(int) <= (kMixedThreads / 32) * kQueue * 2 * sizeof(float4),
               "the compaction's front-hole list lives in the queues' memory");
 
 // w (in units of 2^e_w) -> units of 2^e_tile, sh = e_w - e_tile, round half up
@@ -182,19 +197,24 @@ __device__ __forceinline__ long long rescale(int w, int sh) {
     return sh >= 0 ? (long long)w << sh : (sh > -62 ? ((long long)w + (1ll << (-sh - 1))) >> (-sh) : 0ll);
 }
 
-__global__ void __launch_bounds__(kPushThreads) k_push_mixed(StepParams P) {
+#ifdef PIC_MIXED_MIN_BLOCKS
+#define PIC_MIXED_BOUNDS __launch_bounds__(kMixedThreads, PIC_MIXED_MIN_BLOCKS)
+#else
+#define PIC_MIXED_BOUNDS __launch_bounds__(kMixedThreads)
+#endif
+__global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int sNHoles, sNFront, sNMove;
-    __shared__ double sRed[kPushThreads / 32];
+    __shared__ double sRed[kMixedThreads / 32];
     __shared__ double sQ;
     __shared__ int sTileE;
     __shared__ float sInvQ;
     // two per-warp group buffers: the flush of one iteration's sums runs in the
     // next iteration, after their shared-memory atomics have completed
-    __shared__ int sWarpAcc[kPushThreads / 32][2][kGroups * kSlots];
+    __shared__ int sWarpAcc[kMixedThreads / 32][2][kGroups * kSlots];
     __shared__ int sSlotNode[kSlots];
     // queued segments: {stencil origin node, class bits, start x,y,z, end x,y,z}
-    __shared__ float4 sQueue[kPushThreads / 32][kQueue][2];
+    __shared__ float4 sQueue[kMixedThreads / 32][kQueue][2];
     const Grid &g = P.g;
     const int t = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -600,7 +620,7 @@ cudaError_t launch_push_mixed(const StepParams &p, cudaStream_t s) {
     size_t smem = push_smem_mixed(p.g);
     cudaError_t e = cudaFuncSetAttribute(k_push_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_push_mixed<<<p.g.ntiles, kPushThreads, smem, s>>>(p);
+    k_push_mixed<<<p.g.ntiles, kMixedThreads, smem, s>>>(p);
     return cudaGetLastError();
 }
 

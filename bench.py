@@ -379,10 +379,12 @@ def run_adjoint(args, pkg, dev):
                      "gradient w.r.t. the beam's initial momenta, drift and thermal spread"}
     grads = {}
     base = None
+    starts = {}
     for form in ("fp64", "fp32"):
         sim = make_sim(pkg, cfg, form, dev, 0)
+        starts[form] = sim.particles(ADJ_LOSS["species"])
         if form == "fp64":
-            base = sim.particles(ADJ_LOSS["species"])
+            base = starts[form]
         sim.forward(steps, K)
         g = sim.backward(**ADJ_LOSS)
         t = sim.adjoint_timings()
@@ -392,6 +394,16 @@ def run_adjoint(args, pkg, dev):
                      "backward_over_forward": round(float(t[1] / t[0]), 3),
                      "particle_steps_per_s_forward": round(sim_particles(cfg) * steps / (float(t[0]) / 1e3), 1),
                      "loss": g["loss"], "d_drift_x": float(g["d_drift"][0]), "d_vth": float(g["d_vth"])}
+    # dL/dp0 comes in each handle's own bin order, and the two forms tile the
+    # grid differently: put the FP32 gradient in the FP64 particle order,
+    # matching the same generated particles by (cell, x, y, z)
+    def order(p):
+        return np.lexsort((p["z"], p["y"], p["x"], p["cell"]))
+    o64, o32 = order(starts["fp64"]), order(starts["fp32"])
+    aligned = np.empty_like(grads["fp32"]["d_p0"])
+    aligned[o64] = grads["fp32"]["d_p0"][o32]
+    grads["fp32"]["d_p0"] = aligned
+    out["fp32"]["p0_match_max_dx"] = float(f"{max(np.max(np.abs(starts['fp64'][k][o64] - starts['fp32'][k][o32])) for k in ('x', 'y', 'z')):.3e}")
     keys = ("x", "y", "z", "px", "py", "pz")
 
     def loss_of(dp, eps):

@@ -256,7 +256,12 @@ typedef struct pic_grads {
     double d_drift[3];  /* out: dL/d drift */
     double d_vth;       /* out: dL/d vth = sum_i dL/dp_i . (p_i - drift)/vth */
     int64_t n;          /* in: capacity of d_p0 in particles; out: particles of the species */
-    double *d_p0;       /* in: host array of 3*n doubles (px, py, pz of each particle) or NULL */
+    double *d_p0;       /* in: host array of 3*n doubles (px, py, pz of each particle) or NULL;
+                           particles in the order pic_get_particles gave at the
+                           start of the forward -- this handle's bin order, which
+                           depends on its tiling (the FP32 form tiles z by 12,
+                           the FP64 form by 16), so match particles by their
+                           state, not by index, across handles */
     double reserved[4];
 } pic_grads;
 
