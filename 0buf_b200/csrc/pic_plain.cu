@@ -219,10 +219,28 @@ __device__ __forceinline__ int receivers(double x, int c, int N, double h, int o
     return n;
 }
 
-__global__ void __launch_bounds__(kPushThreads) k_push_plain(StepParams P) {
+// 512 threads, two CTAs per SM: 32 warps per SM at 64 registers (ptxas
+// spills ~200 bytes).  The kernel waits on shared-atomic round trips and FP64
+// dependency chains, and the extra warps hide them: c2 push 208.7 ms against
+// 246.5 ms with 256 threads at 126 registers (320: 229.8, 384: 219.8,
+// 448: 214.5, 256 x 3 CTAs: 218.4)
+#ifndef PIC_PLAIN_THREADS
+#define PIC_PLAIN_THREADS 512
+#endif
+#ifndef PIC_PLAIN_MIN_BLOCKS
+#define PIC_PLAIN_MIN_BLOCKS 2
+#endif
+constexpr int kPlainThreads = PIC_PLAIN_THREADS;  // threads per CTA of k_push_plain
+static_assert(kPlainThreads % 32 == 0, "whole warps");
+#ifdef PIC_PLAIN_MIN_BLOCKS
+#define PIC_PLAIN_BOUNDS __launch_bounds__(kPlainThreads, PIC_PLAIN_MIN_BLOCKS)
+#else
+#define PIC_PLAIN_BOUNDS __launch_bounds__(kPlainThreads)
+#endif
+__global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int sNHoles, sNFront, sNMove;
-    __shared__ double sRed[kPushThreads / 32];
+    __shared__ double sRed[kPlainThreads / 32];
     __shared__ double sQ, sInvQ;
     const Grid &g = P.g;
     const int t = blockIdx.x;
@@ -581,7 +599,7 @@ cudaError_t launch_push_plain(const StepParams &p, cudaStream_t s) {
     size_t smem = push_smem_plain(p.g);
     cudaError_t e = cudaFuncSetAttribute(k_push_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_push_plain<<<p.g.ntiles, kPushThreads, smem, s>>>(p);
+    k_push_plain<<<p.g.ntiles, kPlainThreads, smem, s>>>(p);
     return cudaGetLastError();
 }
 
