@@ -82,7 +82,8 @@ typedef struct pic_config {
     pic_species species[PIC_MAX_SPECIES];
     double capacity_slack;   /* particle slots per tile = count * (1 + slack) + pad; 0 -> 0.25 */
     double outbox_fraction;  /* outbox slots = fraction * total capacity + 65536; 0 -> 0.04 */
-    int tile[3];             /* cells per tile (x, y, z); 0 -> automatic. tile[2] % 4 == 0 */
+    int tile[3];             /* cells per tile (x, y, z); 0 -> automatic: 4 x 4 x 16 (FP64 form),
+                                4 x 4 x 12 (FP32 form), capped by the grid. tile[2] % 4 == 0 */
     int capacity_pad;        /* extra slots per tile; negative -> 64 */
     int reserved[7];
 } pic_config;
