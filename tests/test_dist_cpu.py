@@ -70,3 +70,25 @@ def test_reference_arm_under_torchrun_world2():
     out = json.loads(lines[0])
     assert out["impl"] == "reference" and out["value"] > 0
     assert out["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_bench_particle_matching():
+    """bench.match_particles pairs the same generated particles held by two
+    handles, one with FP32-rounded positions and in another order, including
+    two particles of one cell whose x coincide after FP32 rounding (sorting
+    alone swaps them)."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    rng = np.random.default_rng(1)
+    n = 20000
+    cell = rng.integers(0, 500, n)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    x[0], x[1], y[0], y[1], cell[1] = 0.5, 0.5 + 1e-9, 0.9, 0.1, cell[0]
+    a = dict(cell=cell, x=x, y=y, z=z)
+    perm = rng.permutation(n)
+    b = {k: v[perm].copy() for k, v in a.items()}
+    b["x"] = b["x"].astype(np.float32).astype(np.float64)
+    ia, ib, repaired = bench.match_particles(a, b)
+    assert np.array_equal(perm[ib], ia)
+    assert repaired == 2
