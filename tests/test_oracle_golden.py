@@ -169,3 +169,30 @@ def test_charge_density_totals(oracle_mod):
     m = rng.normal(0, 1, 500)
     r = oracle_mod.charge_density(x, y, z, m, cells, h).reshape(tuple(c + 2 for c in cells))
     np.testing.assert_allclose(r[1:-1, 1:-1, 1:-1].sum(), m.sum(), rtol=1e-12, atol=1e-12)
+
+
+def test_quiet_default_run_bit_exact(oracle_mod, pkg):
+    """The reference's own default run (main.cu:14: 100x4x4 cells, box
+    1.1424 x 0.05 x 0.05, tau 0.001) from its own initial state (the
+    library's quiet start, bit-identical to getUniformMaxwellianParticles):
+    the C restatement reproduces the reference's 10 steps bit for bit on
+    non-cubic cells with about 4000 particles per cell."""
+    d = np.load(os.path.join(GOLDEN, "ref_quiet.npz"))
+    cells = tuple(int(c) for c in d["cells"])
+    sim = oracle_mod.OracleSim(cells, tuple(float(v) for v in d["lengths"]), float(d["tau"]),
+                               threads=os.cpu_count() or 1)
+    st = pkg.quiet_start()
+    for s, name in enumerate(pkg.plasma.QUIET_SORTS):
+        p = st[name]
+        assert sim.add_particles(s, *[p[k] for k in ("x", "y", "z", "px", "py", "pz")], p["m"], p["q_m"]) == p["x"].size
+    for step in range(1, int(d["steps"]) + 1):
+        assert sim.step() == 0
+        assert np.array_equal(sim.cell_counts(), d[f"step{step}_counts"]), step
+        assert sim.energy_reference() == float(d[f"step{step}_energy"]), step
+        if f"step{step}_Ex" in d.files:
+            for f in FIELDS:
+                assert np.array_equal(sim.get_field(f), d[f"step{step}_{f}"]), (step, f)
+    tab = table(sim.particles())
+    tab = tab[np.lexsort((tab[:, 4], tab[:, 3], tab[:, 2], tab[:, 1], tab[:, 0]))]
+    assert tab.shape[0] == int(d["final_rows"])
+    assert np.array_equal(tab[::int(d["sample"])], d["final_particles_sample"])
