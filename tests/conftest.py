@@ -32,3 +32,25 @@ def gpu_available() -> bool:
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def stress_inputs(pkg, cells, lengths, ppc, seed):
+    """The stress configuration's species on a small grid, as
+    tests/golden/make_golden.py makes them for ref_stress.npz (the fixture
+    pins them by a digest): the host generator thinned to the c4 density
+    profile for the profiled species, uniform for the beam.  Returns
+    [(sort, [x, y, z, px, py, pz], m, q_m)]."""
+    import numpy as np
+    counts = pkg.profile_counts(cells, dict(pkg.configs.C4_PROFILE, ppc_mean=ppc)).ravel()
+    cmax = int(counts.max())
+    table = pkg.configs.species_table(ppc, pkg.configs.SPECIES_STRESS)
+    out = []
+    for i, s in enumerate(pkg.configs.SPECIES_STRESS):
+        if "profile" in s:
+            arrs = pkg.host_species(cells, lengths, i, cmax, s["drift"], s["vth"], seed)
+            keep = (np.arange(cmax)[None, :] < counts[:, None]).ravel()
+            arrs = [a[keep] for a in arrs]
+        else:
+            arrs = pkg.host_species(cells, lengths, i, ppc, s["drift"], s["vth"], seed)
+        out.append((s["sort"], arrs, table[i][1], s["q_m"]))
+    return out

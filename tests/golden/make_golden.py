@@ -10,7 +10,10 @@ stored in the fixture (small case) or pinned by a digest (c0 case) so the
 fixtures stand alone; and tests/golden/ref_quiet.npz, the reference's own
 default run (main.cu:14: 100x4x4 cells, box 1.1424 x 0.05 x 0.05, tau 0.001)
 from the reference's own initial state (getUniformMaxwellianParticles,
-maxwell.cu:676-757, pinned by a digest).
+maxwell.cu:676-757, pinned by a digest); and tests/golden/ref_stress.npz, the
+stress configuration's profile and hot electrons (c4's species, dt 0.05) on
+16x8x8 cells, inputs from the host generator thinned to the profile and
+pinned by a digest.
 """
 from __future__ import annotations
 
@@ -112,6 +115,57 @@ def make_c0(steps=10):
     np.savez_compressed(os.path.join(OUT, "ref_c0.npz"), **rec)
 
 
+def stress_inputs(cells, lengths, ppc, seed):
+    """The stress configuration's species on a small grid: the library's host
+    generator (cell-major, keyed by seed, species, cell, slot) thinned to the
+    c4 density profile's per-cell counts for the profiled species (cold ions,
+    hot electrons of vth 0.1), uniform for the beam."""
+    counts = pkg.profile_counts(cells, dict(pkg.configs.C4_PROFILE, ppc_mean=ppc)).ravel()
+    cmax = int(counts.max())
+    table = pkg.configs.species_table(ppc, pkg.configs.SPECIES_STRESS)
+    out = []
+    for i, s in enumerate(pkg.configs.SPECIES_STRESS):
+        if "profile" in s:
+            arrs = pkg.host_species(cells, lengths, i, cmax, s["drift"], s["vth"], seed)
+            keep = (np.arange(cmax)[None, :] < counts[:, None]).ravel()
+            arrs = [a[keep] for a in arrs]
+        else:
+            arrs = pkg.host_species(cells, lengths, i, ppc, s["drift"], s["vth"], seed)
+        out.append((s["sort"], arrs, table[i][1], s["q_m"]))
+    return out
+
+
+STRESS = dict(cells=(16, 8, 8), h=0.1, tau=0.05, ppc=8, seed=3, steps=10)
+
+
+def make_stress():
+    cells, h, tau, ppc, seed, steps = (STRESS[k] for k in ("cells", "h", "tau", "ppc", "seed", "steps"))
+    lengths = tuple(c * h for c in cells)
+    sim = RefSim(cells, lengths, tau, threads=os.cpu_count() or 1)
+    inputs = stress_inputs(cells, lengths, ppc, seed)
+    rec = dict(cells=np.array(cells), h=h, tau=tau, ppc=ppc, seed=seed, steps=steps)
+    rec["inputs_digest"] = digest(np.concatenate([a for _, arrs, _, _ in inputs for a in arrs]))
+    for sort, arrs, m, q_m in inputs:
+        sim.add_particles(sort, *arrs, m, q_m)
+        rec[f"in_s{sort}_count"] = arrs[0].size
+    moved = 0
+    prev = sim.cell_counts()
+    for st in range(1, steps + 1):
+        assert sim.step() == 0
+        c = sim.cell_counts()
+        moved += int(np.abs(c - prev).sum())
+        prev = c
+        for f in FIELDS:
+            rec[f"step{st}_{f}_digest"] = digest(sim.get_field(f))
+        rec[f"step{st}_counts"] = c
+        rec[f"step{st}_energy"] = sim.energy_reference()
+        rec[f"step{st}_particles_digest"] = digest(particle_table(sim.particles()))
+    rec["count_changes"] = moved
+    for f in FIELDS:
+        rec[f"final_{f}"] = sim.get_field(f)
+    np.savez_compressed(os.path.join(OUT, "ref_stress.npz"), **rec)
+
+
 def control_points_dat(path):
     """nt, num and the twelve RMS differences of the reference's
     control_points.dat line (names Ex .. Qz), plus its particle figure."""
@@ -158,7 +212,7 @@ def make_quiet(steps=10):
 if __name__ == "__main__":
     if not RefSim.available():
         sys.exit("oracle/_ref/libref0buf.so missing: run oracle/build_ref.sh where the reference sources exist")
-    which = sys.argv[1:] or ["small", "c0", "quiet"]
+    which = sys.argv[1:] or ["small", "c0", "quiet", "stress"]
     made = []
     if "small" in which:
         make_small()
@@ -169,5 +223,8 @@ if __name__ == "__main__":
     if "quiet" in which:
         make_quiet()
         made.append("ref_quiet.npz")
+    if "stress" in which:
+        make_stress()
+        made.append("ref_stress.npz")
     for f in made:
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")

@@ -83,3 +83,28 @@ def test_stress_adjoint_matches_finite_differences(pkg):
         sim.forward(steps, K)
         g32 = sim.backward(**loss)
     assert abs(g32["d_drift"][0] - fd) / abs(fd) < 1e-3, (g32["d_drift"][0], fd)
+
+
+def test_stress_plain_matches_reference(pkg):
+    """The FP64 plain form in the stress regime (c4's profile, hot electrons,
+    dt 0.05) against the reference's own 10 steps (tests/golden/ref_stress.npz):
+    identical per-cell counts every step, energies and final fields within
+    1e-12."""
+    import os
+    from conftest import GOLDEN, stress_inputs
+    d = np.load(os.path.join(GOLDEN, "ref_stress.npz"))
+    cells, h, tau, ppc = tuple(int(c) for c in d["cells"]), float(d["h"]), float(d["tau"]), int(d["ppc"])
+    lengths = tuple(c * h for c in cells)
+    inputs = stress_inputs(pkg, cells, lengths, ppc, int(d["seed"]))
+    table = [(q_m, m, sort) for sort, _, m, q_m in inputs]
+    with pkg.PicSimulation(cells, lengths, tau, table, precision="fp64") as sim:
+        for sort, arrs, _, _ in inputs:
+            assert sim.load_particles(sort, *arrs) == arrs[0].size
+        for st in range(1, int(d["steps"]) + 1):
+            sim.step(st)
+            assert np.array_equal(sim.cell_counts(), d[f"step{st}_counts"]), st
+            assert sim.energy_reference() == pytest.approx(float(d[f"step{st}_energy"]), rel=1e-12), st
+        for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz", "Qx", "Qy", "Qz"):
+            ref = d[f"final_{f}"]
+            err = np.linalg.norm(sim.get_field(f) - ref) / max(np.linalg.norm(ref), 1e-300)
+            assert err <= 1e-12, (f, err)

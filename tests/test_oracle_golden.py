@@ -196,3 +196,26 @@ def test_quiet_default_run_bit_exact(oracle_mod, pkg):
     tab = tab[np.lexsort((tab[:, 4], tab[:, 3], tab[:, 2], tab[:, 1], tab[:, 0]))]
     assert tab.shape[0] == int(d["final_rows"])
     assert np.array_equal(tab[::int(d["sample"])], d["final_particles_sample"])
+
+
+def test_stress_ten_steps_bit_exact(oracle_mod, pkg):
+    """The stress regime (c4's density profile, cold ions, hot electrons of
+    vth 0.1, dt 0.05; heavy migration) on 16x8x8 cells: the C restatement
+    reproduces the reference's 10 steps bit for bit."""
+    from conftest import stress_inputs
+    d = np.load(os.path.join(GOLDEN, "ref_stress.npz"))
+    cells, h, tau = tuple(int(c) for c in d["cells"]), float(d["h"]), float(d["tau"])
+    lengths = tuple(c * h for c in cells)
+    inputs = stress_inputs(pkg, cells, lengths, int(d["ppc"]), int(d["seed"]))
+    assert digest(np.concatenate([a for _, arrs, _, _ in inputs for a in arrs])) == str(d["inputs_digest"])
+    sim = oracle_mod.OracleSim(cells, lengths, tau, threads=os.cpu_count() or 1)
+    for sort, arrs, m, q_m in inputs:
+        assert sim.add_particles(sort, *arrs, m, q_m) == arrs[0].size
+    assert int(d["count_changes"]) > 1000  # the fixture migrates
+    for st in range(1, int(d["steps"]) + 1):
+        assert sim.step() == 0
+        assert np.array_equal(sim.cell_counts(), d[f"step{st}_counts"]), st
+        assert sim.energy_reference() == float(d[f"step{st}_energy"]), st
+        for f in FIELDS:
+            assert digest(sim.get_field(f)) == str(d[f"step{st}_{f}_digest"]), (st, f)
+        assert digest(table(sim.particles())) == str(d[f"step{st}_particles_digest"]), st
