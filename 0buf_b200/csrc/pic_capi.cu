@@ -606,14 +606,18 @@ int pic_load_particles_cells(pic_handle *h, int species, int64_t n, const int32_
     const int64_t nchunks = (n + kLoadChunk - 1) / kLoadChunk;
     int *icell = nullptr, *tc = nullptr, *stage_cell[2] = {nullptr, nullptr};
     float *off[3] = {nullptr, nullptr, nullptr}, *stage_mom[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    auto drop = [&](auto *&p) {  // free once: release may run again on an error after it
+        dev_free(h, p);
+        p = nullptr;
+    };
     auto release = [&]() {
-        dev_free(h, icell);
-        dev_free(h, tc);
+        drop(icell);
+        drop(tc);
         for (int b = 0; b < 2; b++) {
-            dev_free(h, stage_cell[b]);
-            for (int a = 0; a < 3; a++) dev_free(h, stage_mom[b][a]);
+            drop(stage_cell[b]);
+            for (int a = 0; a < 3; a++) drop(stage_mom[b][a]);
         }
-        for (int a = 0; a < 3; a++) dev_free(h, off[a]);
+        for (int a = 0; a < 3; a++) drop(off[a]);
     };
     auto ck = [&](cudaError_t e, const char *where) {
         if (e == cudaSuccess) return PIC_OK;
