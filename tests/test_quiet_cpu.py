@@ -163,3 +163,12 @@ def test_quiet_start_arguments(pkg):
     w = pkg.quiet_start(n_ions=0)
     q = pkg.quiet_params()
     assert all(w[s]["x"].size == 0 for s in w) and w["beam"]["m"] == -q.rbd / q.lp
+
+
+def test_first_beam_impulse_matches_the_reference_record(pkg):
+    """The reference records the first beam particle's momentum of its default
+    initial state in its source (maxwell.cu:452, and the check at :464):
+    0.20296063288436139.  The quiet start gives it to 2.4e-11 relative (the
+    generator variant with AS 183's textbook remainders would give 0.2215)."""
+    px0 = pkg.quiet_start()["beam"]["px"][0]
+    assert abs(px0 - 0.20296063288436139) <= 1e-10 * 0.20296063288436139
