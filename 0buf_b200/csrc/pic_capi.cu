@@ -66,6 +66,10 @@ StepParams make_params(pic_handle *h) {
     p.outbox = h->outbox;
     p.out_cap = h->out_cap;
     p.st = h->st;
+    if (h->lb_buf) {
+        p.lb_prev = h->lb_buf + h->lb_par * kMaxSpecies;
+        p.lb_cur = (unsigned *)(h->lb_buf + (h->lb_par ^ 1) * kMaxSpecies);
+    }
     return p;
 }
 
@@ -137,6 +141,7 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
     h->sp[s].cap_total = acc;
     h->sp[s].h_start = start;
     h->sp[s].loaded = 1;
+    h->sp[s].lb_known = 0;
     return PIC_OK;
 }
 
@@ -269,12 +274,14 @@ int check_status(pic_handle *h) {
     h->counters[1] = (int64_t)st.dropped;
     h->counters[2] = (int64_t)st.duplicated;
     char msg[200];
-    const unsigned fatal = ST_STENCIL | ST_NAN | ST_BADCELL | ST_OUTBOX;
+    const unsigned fatal = ST_STENCIL | ST_NAN | ST_BADCELL | ST_OUTBOX | ST_TMA;
     if (st.flags & fatal) {
         int code = (st.flags & ST_NAN) ? PIC_ERR_NAN
                    : (st.flags & ST_STENCIL) ? PIC_ERR_STENCIL
-                   : (st.flags & ST_BADCELL) ? PIC_ERR_STATE : PIC_ERR_OUTBOX;
-        snprintf(msg, sizeof(msg), "%s (status flags 0x%x: 1 stencil, 2 outbox, 4 holes, 8 nan, 16 tile full, 32 bins)",
+                   : (st.flags & (ST_BADCELL | ST_TMA)) ? PIC_ERR_STATE : PIC_ERR_OUTBOX;
+        snprintf(msg, sizeof(msg),
+                 "%s (status flags 0x%x: 1 stencil, 2 outbox, 4 holes, 8 nan, 16 tile full, 32 bins, 64 field tile load "
+                 "timed out)",
                  pic_error_string(code), st.flags);
         return set_err(h, code, msg);
     }
@@ -359,10 +366,25 @@ int do_push_deposit(pic_handle *h) {
     size_t nodes = h->g.nodes_pitched();
     for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(h->f[PIC_JX + c], 0, nodes * sizeof(double), h->stream), "zero J");
     CK(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), h->stream), "reset status");
+    if (h->mixed) {
+        // species loaded since the last push: their contribution bound from their momenta
+        float *prev = h->lb_buf + h->lb_par * kMaxSpecies;
+        for (int s = 0; s < h->cfg.nspecies; s++) {
+            if (h->sp[s].lb_known) continue;
+            CK(cudaMemsetAsync(prev + s, 0, sizeof(float), h->stream), "reset bound");
+            CK(contribution_bound_mixed(h->g, h->sp[s].v, h->sp[s].cap_total, (unsigned *)(prev + s), h->stream),
+               "contribution bound");
+            h->launches += 1;
+            h->sp[s].lb_known = 1;
+        }
+        CK(cudaMemsetAsync(h->lb_buf + (h->lb_par ^ 1) * kMaxSpecies, 0, kMaxSpecies * sizeof(float), h->stream),
+           "reset bounds");
+    }
     StepParams p = make_params(h);
     cudaEventRecord(h->ev[2], h->stream);
-    CK(h->mixed ? launch_push_mixed(p, h->stream) : launch_push_plain(p, h->stream), "push_deposit");
+    CK(h->mixed ? launch_push_mixed(p, h->maps, h->stream) : launch_push_plain(p, h->stream), "push_deposit");
     cudaEventRecord(h->ev[3], h->stream);
+    if (h->mixed) h->lb_par ^= 1;
     h->launches += 1;
     h->kin_valid = 1;
     return PIC_OK;
@@ -470,9 +492,8 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
     g.hz = cfg->lz / ((double)cfg->nz);
     g.tx = cfg->tile[0] > 0 ? cfg->tile[0] : std::min(4, g.nx);
     g.ty = cfg->tile[1] > 0 ? cfg->tile[1] : std::min(4, g.ny);
-    // automatic z extent: 16 (plain); 12 in the FP32 form, whose 320-thread
-    // CTAs then fit two per SM in shared memory (measured at c2: push 29.2 ms
-    // against 30.5 ms with 256 threads and 16)
+    // automatic z extent: 16 (plain); 12 in the FP32 form, whose 256-thread
+    // CTAs (an int32 tile current per two warps) then fit two per SM in shared memory
     const int tz_auto = h->mixed ? 12 : 16;
     g.tz = cfg->tile[2] > 0 ? cfg->tile[2] : (g.nz >= tz_auto ? tz_auto : (g.nz + 3) / 4 * 4);
     if (g.tz % 4 != 0 || g.tx < 1 || g.ty < 1 || g.tx > 16 || g.ty > 16 || g.tz > 32) { delete h; return PIC_ERR_ARG; }
@@ -517,6 +538,14 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
         if ((e = cudaMemsetAsync(h->f[fi], 0, nodes * es, h->stream)) != cudaSuccess) return fail(e);
     }
     if ((e = cudaMalloc(&h->dense, g.nodes_ref() * sizeof(double))) != cudaSuccess) return fail(e);
+    if (h->mixed) {
+        if ((e = encode_field_maps(g, (float *const *)&h->f[PIC_EX], (float *const *)&h->f[PIC_HX], &h->maps)) !=
+            cudaSuccess)
+            return fail(e);
+        if ((e = cudaMalloc(&h->lb_buf, 2 * kMaxSpecies * sizeof(float))) != cudaSuccess) return fail(e);
+        if ((e = cudaMemsetAsync(h->lb_buf, 0, 2 * kMaxSpecies * sizeof(float), h->stream)) != cudaSuccess)
+            return fail(e);
+    }
     if ((e = cudaMalloc(&h->st, sizeof(DevStatus))) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(h->st, 0, sizeof(DevStatus), h->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaMallocHost(&h->st_host, sizeof(DevStatus))) != cudaSuccess) return fail(e);
@@ -544,6 +573,7 @@ int pic_destroy(pic_handle *h) {
     if (h->dred) cudaFree(h->dred);
     if (h->hred) cudaFreeHost(h->hred);
     if (h->dcounts) cudaFree(h->dcounts);
+    if (h->lb_buf) cudaFree(h->lb_buf);
     double *diag[3] = {h->rho, h->gauss, h->gauss0};
     for (double *d : diag)
         if (d) cudaFree(d);

@@ -30,6 +30,9 @@ struct pic_handle {
         // per-tile cell sort writes into before the two sets swap
         int *alt_cell;
         float *alt[6];
+        // FP32 form: the bound of its contributions is known from a push
+        // (cleared whenever the bins are rebuilt)
+        int lb_known;
     } sp[pic::kMaxSpecies];
     int64_t sorts;  // tile sorts run by the last step
     void *outbox;
@@ -60,6 +63,12 @@ struct pic_handle {
     // places and scatters the previous chunk
     cudaStream_t copy_stream;
     cudaEvent_t lev[5];
+    // FP32 form: TMA descriptors of the E/H arrays (encoded once: the field
+    // arrays never move) and the per-species contribution bounds of the last
+    // two pushes (2 x PIC_MAX_SPECIES floats; lb_par selects the previous half)
+    pic::MixedMaps maps;
+    float *lb_buf;
+    int lb_par;
 };
 
 namespace pic_host {

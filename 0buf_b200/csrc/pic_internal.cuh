@@ -16,6 +16,7 @@
 //            index; only tile leavers move (outbox -> insert).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "pic0buf.h"
@@ -34,6 +35,7 @@ enum : unsigned {
     ST_NAN = 8u,         // non-finite momentum
     ST_TILE_FULL = 16u,  // arrivals did not fit their tile (kept in the outbox, rebin needed)
     ST_BADCELL = 32u,    // a bin held a cell outside its tile, or the compaction did not pair up
+    ST_TMA = 64u,        // the field tile's TMA load did not complete within the wait limit
 };
 
 struct DevStatus {
@@ -154,6 +156,18 @@ struct StepParams {
     void *outbox;
     unsigned out_cap;
     DevStatus *st;
+    // mixed push: per species, the largest contribution bound of the last
+    // push (float, 0 = none yet) and the one this push records (float bits,
+    // atomicMax); sizes the int32 tile current's quantum
+    const float *lb_prev;
+    unsigned *lb_cur;
+};
+
+// FP32 form: TMA descriptors of the six E/H field arrays (3D {Nz+2, Ny+2,
+// Nx+2} FP32 with the pitched z row, box = one tile + halo); a kernel
+// parameter (__grid_constant__), so the descriptors live in parameter space
+struct MixedMaps {
+    CUtensorMap m[6];
 };
 
 

@@ -24,7 +24,11 @@ void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], dou
 size_t push_smem_mixed(const Grid &g);
 // dynamic + static shared memory of the mixed push kernel ((size_t)-1 if it cannot be queried)
 size_t push_smem_total_mixed(const Grid &g);
-cudaError_t launch_push_mixed(const StepParams &p, cudaStream_t s);
+cudaError_t launch_push_mixed(const StepParams &p, const MixedMaps &maps, cudaStream_t s);
+// largest contribution bound of a species' particles from their momenta (float bits, atomicMax into *out)
+cudaError_t contribution_bound_mixed(const Grid &g, const SpeciesView &S, int64_t cap, unsigned *out, cudaStream_t s);
+// TMA descriptors of the FP32 E/H arrays for the push's field tile
+cudaError_t encode_field_maps(const Grid &g, float *const E[3], float *const H[3], MixedMaps *maps);
 
 // form-independent (pic_common.cu, FP64 parts with -fmad=false)
 cudaError_t launch_insert(const StepParams &p, cudaStream_t s);

@@ -6,8 +6,11 @@
 // FP32 momentum).  Push, deposit and Yee run in FP32; the deposit
 // pre-reduces each tile's current in shared memory (64-bit fixed point, see
 // fx_add) and adds the tile into the global J in FP64.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <algorithm>
 #include "pic_internal.cuh"
 #include "pic_kernels.cuh"
 
@@ -56,11 +59,10 @@ __global__ void k_e_update_mixed(Grid g, float *Ex, float *Ey, float *Ez, const 
 // Interpolate3D (cell.h:1054-1153) in cell units on the FP32 tile, stored as
 // yz-quads: Q[n] = (T[n], T[n+dz], T[n+dy], T[n+dy+dz]), so the 8 taps are two
 // 128-bit shared loads (the same products and sums, in the same order, as
-// the 8 scalar taps)
-__device__ __forceinline__ float interp_mixed(const float4 *__restrict__ Q, int SY, int SZ, int n0, int i, int l,
-                                              int k, float sx, float sy, float sz) {
-    const int n = n0 + (i * SY + l) * SZ + k;
-    const float4 A = Q[n], B = Q[n + SY * SZ];
+// the 8 scalar taps).  Q points at the stencil's lower node; the upper x node
+// is SYZ quads further; sx, sy, sz weight the lower node of each axis.
+__device__ __forceinline__ float interp_quad(const float4 *__restrict__ Q, int SYZ, float sx, float sy, float sz) {
+    const float4 A = Q[0], B = Q[SYZ];
     const float sx1 = 1.f - sx, sy1 = 1.f - sy, sz1 = 1.f - sz;
     float t1 = sx * (sy * (sz * A.x + sz1 * A.y) + sy1 * (sz * A.z + sz1 * A.w));
     float t2 = sx1 * (sy * (sz * B.x + sz1 * B.y) + sy1 * (sz * B.z + sz1 * B.w));
@@ -155,30 +157,66 @@ __device__ __forceinline__ PartM load_part(const SpeciesView &S, int slot) {
     return p;
 }
 
-// Deposit of the warp's current, two levels:
-//  1. the depositing lanes form one group per distinct cell (match.any); for
-//     up to kGroups groups per warp, lanes add the first zigzag segment of
-//     their particle into a per-warp int32 scratch of 54 node slots per group
-//     -- the nodes that the segments of a particle in one cell can reach (Jx
-//     2x3x3, Jy 3x2x3, Jz 3x3x2 around the cell's stencil origin) -- with
-//     native 32-bit shared atomics.  The warp's quantum q_w is a power of two
-//     above 2^-22 x the largest possible contribution of any of its lanes
-//     (1.0834 |current of the full step|, reduced with redux.sync), so the
-//     int32 sums of <= 32 contributions cannot overflow.  The <= 54 sums per
-//     group then go into the tile's exact 64-bit fixed-point J (fx_add).
-//  2. segments that do not fit that pattern -- the second segment of a
-//     particle that crosses a cell-centre plane, and both segments of a lane
-//     beyond kGroups distinct cells (bins out of cell order) -- are queued
-//     per warp and deposited 32 at a time, one per lane, straight into the
-//     tile J, so a few such lanes do not stall the other lanes of their warp.
-constexpr int kGroups = 4;
-constexpr int kSlots = 54;
-// 320 threads, two CTAs per SM (96 registers, no spills): 20 warps per SM
-// against 16 with 256 threads at 123 registers; the kernel is issue-bound and
-// the extra warps cut the c2 push from 30.5 to 29.2 ms (288 and 384 threads
-// measured slower)
+// ------------------------------------------------- tensor-memory staging --
+// The CTA's field tile (6 components, tile + 2-node halo, plus one row in y
+// and z for the quads) arrives by six 3D TMA loads (cp.async.bulk.tensor,
+// no multicast: every tensor map covers this GPU's own field arrays) into a
+// raw staging area, completing on one mbarrier.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int c0,
+                                            int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+// try_wait suspends for a bounded time per call; 2^20 calls bound the wait
+// far above any real TMA latency, after which the CTA reports ST_TMA
+constexpr int kTmaWaitLimit = 1 << 20;
+
+// Deposit of the tile current, two levels:
+//  1. the first zigzag segment of every particle goes, with native int32
+//     shared-memory atomics, into a tile-sized int32 current that two warps
+//     share (kJCopies per CTA).  Its quantum q_s = 2^e_s is static per
+//     species: cmax bounds one contribution (twice the largest of the species
+//     in the last push, or from its momenta before its first push; at most
+//     the light-speed bound) and q_s >= 2^-22 cmax keeps the FMA
+//     magic-number rounding of a contribution exact.  Each warp adds up, per
+//     iteration, the bounds of its lanes' contributions (redux.sync): its
+//     share of any node's int32 sum never exceeds that running total.  Before
+//     the total could pass 2^30 the warp moves the current into the tile's
+//     exact 64-bit fixed-point J (atomicExch, so the other warp's concurrent
+//     adds are never lost; rescaled exactly: both quanta are powers of two)
+//     and starts its total again at zero, so two warps' shares stay below
+//     2^31.  At the end of the species the copies are summed per node into
+//     the tile J.
+//  2. the second segment of a particle that crosses a cell-centre plane
+//     (1-4% of particles), and both segments of a particle whose contribution
+//     bound exceeds cmax, are queued per warp and deposited 32 at a time, one
+//     per lane, straight into the 64-bit tile J, so a few such lanes do not
+//     stall the other lanes of their warp.
+// No cell grouping: the bins need not be in cell order.
 #ifndef PIC_MIXED_THREADS
-#define PIC_MIXED_THREADS 320
+#define PIC_MIXED_THREADS 256
 #endif
 #ifndef PIC_MIXED_MIN_BLOCKS
 #define PIC_MIXED_MIN_BLOCKS 2
@@ -187,49 +225,79 @@ constexpr int kSlots = 54;
 #define PIC_MIXED_QUEUE 64
 #endif
 constexpr int kMixedThreads = PIC_MIXED_THREADS;  // threads per CTA of k_push_mixed
+constexpr int kMixedWarps = kMixedThreads / 32;
+constexpr int kJCopies = kMixedWarps / 2;         // int32 tile currents per CTA: one per two warps
 constexpr int kQueue = PIC_MIXED_QUEUE;           // queued segments per warp
 static_assert(kMixedThreads % 32 == 0, "whole warps");
-static_assert(kHoleMax * sizeof(int) <= (kMixedThreads / 32) * kQueue * 2 * sizeof(float4),
+static_assert(kQueue >= 64, "one iteration can queue two segments per lane");
+static_assert(kHoleMax * sizeof(int) <= kMixedWarps * kQueue * 2 * sizeof(float4),
               "the compaction's front-hole list lives in the queues' memory");
 
 // w (in units of 2^e_w) -> units of 2^e_tile, sh = e_w - e_tile, round half up
-__device__ __forceinline__ long long rescale(int w, int sh) {
-    return sh >= 0 ? (long long)w << sh : (sh > -62 ? ((long long)w + (1ll << (-sh - 1))) >> (-sh) : 0ll);
+__device__ __forceinline__ long long rescale(long long w, int sh) {
+    return sh >= 0 ? w << sh : (sh > -62 ? (w + (1ll << (-sh - 1))) >> (-sh) : 0ll);
 }
 
-#ifdef PIC_MIXED_MIN_BLOCKS
+// shared-memory layout of k_push_mixed (dynamic part), byte offsets
+struct MixedSmem {
+    size_t raw, raw_comp, quads, jw, tilej, holes, total;
+};
+__host__ __device__ inline size_t round_up_sz(size_t v, size_t a) { return (v + a - 1) / a * a; }
+__host__ __device__ inline MixedSmem mixed_smem(int tx, int ty, int tz) {
+    MixedSmem m;
+    const size_t SX = tx + 2, SY = ty + 2, SZ = tz + 2, nn = SX * SY * SZ;
+    const size_t box = (size_t)(tx + 2) * (ty + 3) * (tz + 4);  // TMA box of one component
+    m.raw_comp = round_up_sz(box * sizeof(float), 128);
+    const size_t raw_bytes = 6 * m.raw_comp;
+    const size_t jw_bytes = (size_t)kJCopies * 3 * nn * sizeof(int);
+    // the raw TMA staging area is consumed (into the quads) before the int32
+    // currents are cleared, so the two share memory
+    m.raw = 0;
+    m.jw = 0;
+    m.quads = round_up_sz(raw_bytes > jw_bytes ? raw_bytes : jw_bytes, 128);
+    m.tilej = m.quads + 6 * nn * sizeof(float4);
+    m.holes = m.tilej + 3 * nn * sizeof(unsigned long long);
+    m.total = m.holes + kHoleMax * sizeof(int);
+    return m;
+}
+
 #define PIC_MIXED_BOUNDS __launch_bounds__(kMixedThreads, PIC_MIXED_MIN_BLOCKS)
-#else
-#define PIC_MIXED_BOUNDS __launch_bounds__(kMixedThreads)
-#endif
-__global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps maps, StepParams P) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long sBar;
     __shared__ int sNHoles, sNFront, sNMove;
-    __shared__ double sRed[kMixedThreads / 32];
+    __shared__ double sRed[kMixedWarps];
+    __shared__ unsigned sLbMax;
     __shared__ double sQ;
     __shared__ int sTileE;
     __shared__ float sInvQ;
-    // two per-warp group buffers: the flush of one iteration's sums runs in the
-    // next iteration, after their shared-memory atomics have completed
-    __shared__ int sWarpAcc[kMixedThreads / 32][2][kGroups * kSlots];
-    __shared__ int sSlotNode[kSlots];
     // queued segments: {stencil origin node, class bits, start x,y,z, end x,y,z}
-    __shared__ float4 sQueue[kMixedThreads / 32][kQueue][2];
+    __shared__ float4 sQueue[kMixedWarps][kQueue][2];
     const Grid &g = P.g;
     const int t = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
+    const unsigned lt = (1u << lane) - 1;
     const int tk = t % g.ntz, tl = (t / g.ntz) % g.nty, ti = t / (g.ntz * g.nty);
     const int i0 = ti * g.tx, l0 = tl * g.ty, k0 = tk * g.tz;
     const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
-    const int nn = SX * SY * SZ;
-    // FP32 field tile as yz-quads first (16-byte aligned), then the fixed-point tile J
-    float4 *sF = (float4 *)smem_raw;  // Ex Ey Ez Hx Hy Hz
-    unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);
-    int *sHoles = (int *)(sJ + 3 * nn);
+    const int SYZ = SY * SZ;
+    const int nn = SX * SYZ;
+    const int BY = g.ty + 3, BZ = g.tz + 4;
+    const MixedSmem L = mixed_smem(g.tx, g.ty, g.tz);
+    float4 *sF = (float4 *)(smem_raw + L.quads);  // Ex Ey Ez Hx Hy Hz as yz-quads
+    unsigned long long *sJ = (unsigned long long *)(smem_raw + L.tilej);
+    int *sJw = (int *)(smem_raw + L.jw);
+    int *sHoles = (int *)(smem_raw + L.holes);
     // the front-hole list of the compaction reuses the (then drained) queues
     int *sFront = (int *)&sQueue[0][0][0];
-    int *wacc = &sWarpAcc[warp][0][0];
+    int *myJ = sJw + (warp % kJCopies) * 3 * nn;
+
+    // a TMA destination starts on a 128-byte boundary (block-uniform check)
+    if (smem_u32(smem_raw + L.raw) & 127u) {
+        if (threadIdx.x == 0) atomicOr(&P.st->flags, ST_TMA);
+        return;
+    }
     if (threadIdx.x == 0) {
         // quantum of the fixed-point tile J (see fx_add): |contribution| < 1.0834 |m| per segment
         double bound = 0.0;
@@ -239,44 +307,40 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
         sQ = ldexp(1.0, e2 - 62);
         sTileE = e2 - 62;  // tile quantum 2^(e2-62)
         sInvQ = (float)ldexp(1.0, 62 - e2);
+        mbar_init(&sBar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    for (int e = lane; e < 2 * kGroups * kSlots; e += 32) wacc[e] = 0;
-    if (threadIdx.x < kSlots) {
-        // slot -> tile-local node offset from a cell's stencil origin (local index 0,0,0)
-        const int e = threadIdx.x;
-        int comp, a, b, c;
-        if (e < 18) { comp = 0; a = e / 9; b = (e / 3) % 3; c = e % 3; }
-        else if (e < 36) { comp = 1; a = (e - 18) / 6; b = ((e - 18) / 3) % 2; c = (e - 18) % 3; }
-        else { comp = 2; a = (e - 36) / 6; b = ((e - 36) / 2) % 3; c = (e - 36) % 2; }
-        sSlotNode[e] = comp * nn + ((2 + a) * SY + (2 + b)) * SZ + (2 + c);
-    }
-
-    const float *const *E = (const float *const *)P.E;
-    const float *const *H = (const float *const *)P.H;
-    const float *Fsrc[6] = {E[0], E[1], E[2], H[0], H[1], H[2]};
-    for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
-        const int c = idx % SZ, b = (idx / SZ) % SY, a = idx / (SZ * SY);
-        const int gi = i0 + a, gl = l0 + b, gk = k0 + c;
-        // taps outside the staged tile or the field arrays are never read: 0
-        const bool in00 = gi < g.NX && gl < g.NY && gk < g.NZ;
-        const bool in01 = in00 && c + 1 < SZ && gk + 1 < g.NZ;
-        const bool in10 = in00 && b + 1 < SY && gl + 1 < g.NY;
-        const bool in11 = in01 && in10;
-        const size_t n = in00 ? g.node(gi, gl, gk) : 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned comp_bytes = (unsigned)((size_t)(g.tx + 2) * BY * BZ * sizeof(float));
+        mbar_arrive_expect_tx(&sBar, 6 * comp_bytes);
 #pragma unroll
-        for (int f = 0; f < 6; f++) {
-            const float *F = Fsrc[f];
-            sF[f * nn + idx] = make_float4(in00 ? F[n] : 0.f, in01 ? F[n + 1] : 0.f, in10 ? F[n + g.pz] : 0.f,
-                                           in11 ? F[n + g.pz + 1] : 0.f);
-        }
-        sJ[idx] = 0ull;
-        sJ[nn + idx] = 0ull;
-        sJ[2 * nn + idx] = 0ull;
+        for (int f = 0; f < 6; f++)
+            tma_load_3d(smem_raw + L.raw + f * L.raw_comp, &maps.m[f], &sBar, k0, l0, i0);
     }
+    for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) sJ[idx] = 0ull;
+    bool staged = false;
+    for (int it = 0; it < kTmaWaitLimit && !(staged = mbar_try_wait(&sBar, 0)); it++) {
+    }
+    if (!__syncthreads_and(staged)) {
+        if (threadIdx.x == 0) atomicOr(&P.st->flags, ST_TMA);
+        return;
+    }
+    // raw [a][b][c] (c fastest, extents SX, BY, BZ) -> yz-quads
+    // Q[n] = (T[n], T[n+dz], T[n+dy], T[n+dy+dz]); out-of-array taps arrive as 0
+    for (int idx = threadIdx.x; idx < 6 * nn; idx += blockDim.x) {
+        const int f = idx / nn, r = idx - f * nn;
+        const int a = r / SYZ, bc = r - a * SYZ, b = bc / SZ, c = bc - b * SZ;
+        const float *R = (const float *)(smem_raw + L.raw + f * L.raw_comp) + (a * BY + b) * BZ + c;
+        sF[idx] = make_float4(R[0], R[1], R[BZ], R[BZ + 1]);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kJCopies * 3 * nn; idx += blockDim.x) sJw[idx] = 0;
+    if (threadIdx.x == 0) sLbMax = 0u;
     __syncthreads();
     const float inv_q = sInvQ;
     const int tile_e = sTileE;
-    const int slotA = sSlotNode[lane], slotB = lane < kSlots - 32 ? sSlotNode[32 + lane] : 0;
     float4(*queue)[2] = sQueue[warp];
 
     const float ctx = (float)(g.tau / g.hx), cty = (float)(g.tau / g.hy), ctz = (float)(g.tau / g.hz);
@@ -293,10 +357,31 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
         const double M = S.m / S.q_m;
         // per-species deposit weights a*h/tau (see pqr_mixed)
         const float wx = (float)(S.m * g.hx / g.tau), wy = (float)(S.m * g.hy / g.tau), wz = (float)(S.m * g.hz / g.tau);
+        // contribution bound of the int32 path: twice the last push's largest,
+        // else the light-speed bound (|v| < c: |dx| < tau/h per axis)
+        const float light = 1.0834f * fmaxf(fabsf(wx) * ctx, fmaxf(fabsf(wy) * cty, fabsf(wz) * ctz));
+        const float prev = P.lb_prev ? P.lb_prev[s] : 0.f;
+        const float cmax = prev > 0.f ? fminf(2.f * prev, light) : light;
+        // int32 quantum 2^e_s >= 2^-22 cmax
+        const int e_s = max(exponent_above(cmax * 0x1p-22f), -100);
+        const float inv_qs = pow2f(-e_s);
+        const int sh = e_s - tile_e;  // int32 quantum / tile quantum = 2^sh
+        // running bound of this warp's share of any node's int32 sum, in quanta
+        unsigned run = 0;
+        auto flush_current = [&]() {
+            __syncwarp();
+            for (int idx = lane; idx < 3 * nn; idx += 32) {
+                if (myJ[idx]) {
+                    const int w = atomicExch(&myJ[idx], 0);
+                    if (w) atomicAdd(&sJ[idx], (unsigned long long)rescale(w, sh));
+                }
+            }
+            __syncwarp();
+        };
         if (threadIdx.x == 0) { sNHoles = 0; sNFront = 0; sNMove = 0; }
         __syncthreads();
-        unsigned unsorted = 0;
         int qn = 0;  // segments in this warp's queue (warp-uniform)
+        float lbmax = 0.f;
         // deposit the queued segments [from, from + n), one per lane, into the tile J
         auto drain_range = [&](int from, int n) {
             if (lane < n) {
@@ -312,37 +397,6 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
             }
             __syncwarp();
         };
-        auto drain = [&](int n) { drain_range(0, n); };
-        auto drain_top32 = [&](int n) { drain_range(n - 32, 32); };
-        // add the group sums of buffer buf (groups led by the lanes of lead, stencil
-        // origins n0v, warp/tile quantum shift shv) into the tile J and clear them;
-        // exact: both quanta are powers of two, the tile bound keeps the sum below 2^62
-        auto flush_groups = [&](int *buf, unsigned lead, int n0v, int shv) {
-            unsigned lm = lead;
-            for (int gi = 0; gi < kGroups && lm; gi++) {
-                const int ld = __ffs(lm) - 1;
-                lm &= lm - 1;
-                const int base = __shfl_sync(FULL, n0v, ld);
-                int *wg = buf + gi * kSlots;
-                int w = wg[lane];
-                if (w) {
-                    wg[lane] = 0;
-                    const long long add = rescale(w, shv);
-                    if (add) atomicAdd(&sJ[base + slotA], (unsigned long long)add);
-                }
-                if (lane < kSlots - 32) {
-                    w = wg[32 + lane];
-                    if (w) {
-                        wg[32 + lane] = 0;
-                        const long long add = rescale(w, shv);
-                        if (add) atomicAdd(&sJ[base + slotB], (unsigned long long)add);
-                    }
-                }
-            }
-        };
-        int gbuf = 0;  // buffer of this iteration's sums; the other one holds the pending ones
-        unsigned pend_lead = 0;
-        int pend_n0 = 0, pend_sh = 0;
         // warp-synchronous loop: every lane of a warp runs the same iterations;
         // the next particle is loaded before the current one is processed
         const int stride = blockDim.x;
@@ -364,24 +418,27 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
                     i = i0; l = l0; k = k0;
                 }
             }
-            // tile-local node of reference tile index (0,0,0): cell_local - 2
-            const int n0 = ((i - i0 - 2) * SY + (l - l0 - 2)) * SZ + (k - k0 - 2);
+            // tile-local node of the particle's cell and of reference tile index (0,0,0)
+            const int lc = ((i - i0) * SY + (l - l0)) * SZ + (k - k0);
+            const int n0 = lc - 2 * (SYZ + SZ + 1);
             float xs[3] = {cur.x, cur.y, cur.z};
             if (!active) xs[0] = xs[1] = xs[2] = 0.25f;
             float pu = active ? cur.px : 0.f, pv = active ? cur.py : 0.f, pw = active ? cur.pz : 0.f;
 
             // ---- GetField (cell.h:1257-1290) in cell units: getCellNumber = 2,
             // getCellNumberCenter = 2 + (offset >= 1/2), weights s1 = 1-o, s2 = 1/2-o (+1)
-            const int i1x = 2 + (xs[0] >= 0.5f), i1y = 2 + (xs[1] >= 0.5f), i1z = 2 + (xs[2] >= 0.5f);
-            const float s1 = 1.f - xs[0], s2 = (i1x == 2 ? 0.5f : 1.5f) - xs[0];
-            const float s3 = 1.f - xs[1], s4 = (i1y == 2 ? 0.5f : 1.5f) - xs[1];
-            const float s5 = 1.f - xs[2], s6 = (i1z == 2 ? 0.5f : 1.5f) - xs[2];
-            float fEx = interp_mixed(sF, SY, SZ, n0, 2, i1y, i1z, s1, s4, s6);
-            float fEy = interp_mixed(sF + nn, SY, SZ, n0, i1x, 2, i1z, s2, s3, s6);
-            float fEz = interp_mixed(sF + 2 * nn, SY, SZ, n0, i1x, i1y, 2, s2, s4, s5);
-            float fHx = interp_mixed(sF + 3 * nn, SY, SZ, n0, i1x, 2, 2, s2, s3, s5);
-            float fHy = interp_mixed(sF + 4 * nn, SY, SZ, n0, 2, i1y, 2, s1, s4, s5);
-            float fHz = interp_mixed(sF + 5 * nn, SY, SZ, n0, 2, 2, i1z, s1, s3, s6);
+            const int cx = xs[0] >= 0.5f, cy = xs[1] >= 0.5f, cz = xs[2] >= 0.5f;
+            const int i1x = 2 + cx, i1y = 2 + cy, i1z = 2 + cz;
+            const float s1 = 1.f - xs[0], s2 = (cx ? 1.5f : 0.5f) - xs[0];
+            const float s3 = 1.f - xs[1], s4 = (cy ? 1.5f : 0.5f) - xs[1];
+            const float s5 = 1.f - xs[2], s6 = (cz ? 1.5f : 0.5f) - xs[2];
+            const int ox = cx * SYZ, oy = cy * SZ, oz = cz;
+            float fEx = interp_quad(sF + lc + oy + oz, SYZ, s1, s4, s6);
+            float fEy = interp_quad(sF + nn + lc + ox + oz, SYZ, s2, s3, s6);
+            float fEz = interp_quad(sF + 2 * nn + lc + ox + oy, SYZ, s2, s4, s5);
+            float fHx = interp_quad(sF + 3 * nn + lc + ox, SYZ, s2, s3, s5);
+            float fHy = interp_quad(sF + 4 * nn + lc + oy, SYZ, s1, s4, s5);
+            float fHz = interp_quad(sF + 5 * nn + lc + oz, SYZ, s1, s3, s6);
 
             // ---- Particle::Move (particle.h:65-202), FP32
             pu += tau1 * fEx;
@@ -424,58 +481,53 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
                 bad |= ST_STENCIL;
                 dep = false;
             }
-            // warp quantum: 2^(ew-22) with 2^(ew-1) <= wmax < 2^ew, wmax the largest
-            // contribution bound of the warp's lanes (1.0834 |current of the full
-            // step|, redux.sync max).  Contributions then scale to |w| < 2^22, so the
-            // FMA magic-number rounding below is exact, and 64 of them sum below 2^28.
+            // contribution bound of this particle (1.0834 |current of the full step|)
             const float lb = dep ? 1.0834f * fmaxf(fabsf(wx * (xe[0] - xs[0])),
                                                    fmaxf(fabsf(wy * (xe[1] - xs[1])), fabsf(wz * (xe[2] - xs[2]))))
                                  : 0.f;
-            const float wmax = __uint_as_float(__reduce_max_sync(FULL, __float_as_uint(lb)));
-            const int ew = max(exponent_above(wmax), -100);
-            const float inv_qw = pow2f(22 - ew);
-            const int sh = ew - 22 - tile_e;  // warp quantum / tile quantum = 2^sh
-            // one group per distinct cell among the depositing lanes
-            const unsigned same = __match_any_sync(FULL, dep ? cur.cell : -1);
-            const int leader = __ffs(same) - 1;
-            const unsigned leaders = __ballot_sync(FULL, dep && lane == leader);
-            const int grp = __popc(leaders & ((1u << leader) - 1));
-            const bool fast = dep && grp < kGroups;
-            unsorted += dep && !fast;
+            lbmax = fmaxf(lbmax, lb);
+            const bool fast = dep && lb <= cmax;
+            {
+                // |round(v/q_s)| <= lb/q_s + 1/2 per contribution, one contribution per node and lane
+                const unsigned add = __reduce_add_sync(FULL, fast ? (unsigned)(lb * inv_qs) + 1u : 0u);
+                if (run + add > 0x40000000u) {
+                    flush_current();
+                    run = 0;
+                }
+                run += add;
+            }
             // the second zigzag segment exists only where a cell-centre plane is crossed
             const bool cross = dep && (i2[0] != i1x || i2[1] != i1y || i2[2] != i1z);
             float x2[3] = {xe[0], xe[1], xe[2]};
             if (cross) split_point(i1, i2, xs, xe, x2);
-            flush_groups(wacc + (gbuf ^ 1) * (kGroups * kSlots), pend_lead, pend_n0, pend_sh);
             if (fast) {
                 float v[12];
                 pqr_mixed(i1, xs, x2, wx, wy, wz, v);
-                int *wb = wacc + gbuf * (kGroups * kSlots) + grp * kSlots;
-                const int cx = i1x - 2, cy = i1y - 2, cz = i1z - 2;
-                const int bx = cx * 9 + cy * 3 + cz, by = 18 + cx * 6 + cy * 3 + cz, bz = 36 + cx * 6 + cy * 2 + cz;
-                const int off[12] = {bx, bx + 1, bx + 3, bx + 4, by, by + 1, by + 6, by + 7, bz, bz + 2, bz + 6, bz + 8};
+                // Jx (0,0,0) (0,0,1) (0,1,0) (0,1,1); Jy (0,0,0) (0,0,1) (1,0,0) (1,0,1);
+                // Jz (0,0,0) (0,1,0) (1,0,0) (1,1,0) from the base node iv = i1
+                int *J = myJ + lc + ox + oy + oz;
+                const int off[12] = {0, 1, SZ, SZ + 1, nn, nn + 1, nn + SYZ, nn + SYZ + 1,
+                                     2 * nn, 2 * nn + SZ, 2 * nn + SYZ, 2 * nn + SYZ + SZ};
 #pragma unroll
                 for (int q = 0; q < 12; q++) {
-                    int w = __float_as_int(fmaf(v[q], inv_qw, 12582912.0f)) - 0x4B400000;  // round(v/q_w)
-                    if (w) atomicAdd(&wb[off[q]], w);
+                    const int w = __float_as_int(fmaf(v[q], inv_qs, 12582912.0f)) - 0x4B400000;  // round(v/q_s)
+                    if (w) atomicAdd(J + off[q], w);
                 }
             }
             // queue the other segments (warp-aggregated positions)
             {
                 const bool t1 = dep && !fast, t2 = cross;
                 const unsigned b1 = __ballot_sync(FULL, t1), b2 = __ballot_sync(FULL, t2);
-                const unsigned lt = (1u << lane) - 1;
                 const int ntask = __popc(b1) + __popc(b2);
                 if (ntask) {
                     if (qn + ntask > kQueue) {
-                        drain(qn);
+                        drain_range(0, qn);
                         qn = 0;
                     }
                     int pos = qn + __popc(b1 & lt) + __popc(b2 & lt);
                     const float n0f = __int_as_float(n0);
                     if (t1) {
-                        queue[pos][0] = make_float4(n0f, __int_as_float((i1x - 2) | ((i1y - 2) << 1) | ((i1z - 2) << 2)),
-                                                    xs[0], xs[1]);
+                        queue[pos][0] = make_float4(n0f, __int_as_float(cx | (cy << 1) | (cz << 2)), xs[0], xs[1]);
                         queue[pos][1] = make_float4(xs[2], x2[0], x2[1], x2[2]);
                         pos += t2;
                     }
@@ -487,18 +539,12 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
                     qn += ntask;
                     if (qn >= 32) {
                         __syncwarp();
-                        drain_top32(qn);
+                        drain_range(qn - 32, 32);
                         qn -= 32;
                     }
                 }
             }
-            pend_lead = leaders;
-            pend_n0 = n0;
-            pend_sh = sh;
-            gbuf ^= 1;
-            __syncwarp();
 
-            if (!active) continue;
             // ---- new cell (Reflect cell.h:1427-1478 and migration, in cell units)
             int ci[3] = {i, l, k};
             const int nc[3] = {g.nx, g.ny, g.nz};
@@ -514,43 +560,74 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
                 xe[d] = fminf(fmaxf(xe[d], 0.f), kOneBelow);
             }
             const int newcell = g.cell_of(ci[0], ci[1], ci[2]);
-            if ((unsigned)(ci[0] - i0) < (unsigned)g.tx && (unsigned)(ci[1] - l0) < (unsigned)g.ty &&
-                (unsigned)(ci[2] - k0) < (unsigned)g.tz) {
+            const bool stay = (unsigned)(ci[0] - i0) < (unsigned)g.tx && (unsigned)(ci[1] - l0) < (unsigned)g.ty &&
+                              (unsigned)(ci[2] - k0) < (unsigned)g.tz;
+            if (active && stay) {
                 S.cell[slot] = newcell;
                 S.ox[slot] = xe[0]; S.oy[slot] = xe[1]; S.oz[slot] = xe[2];
                 S.fx[slot] = pu; S.fy[slot] = pv; S.fz[slot] = pw;
-            } else {
-                unsigned e = atomicAdd(&P.st->out_count, 1u);
-                if (e < P.out_cap) {
-                    OutMixed o;
-                    o.ox = xe[0]; o.oy = xe[1]; o.oz = xe[2]; o.px = pu; o.py = pv; o.pz = pw;
-                    o.cell = newcell;
-                    o.species = s;
-                    outbox[e] = o;
-                    moved++;
-                } else {
-                    bad |= ST_OUTBOX;
+            }
+            // leavers: one outbox and one hole-list reservation per warp
+            const bool leave = active && !stay;
+            const unsigned lm = __ballot_sync(FULL, leave);
+            if (lm) {
+                const int nl = __popc(lm), rank = __popc(lm & lt);
+                unsigned obase = 0;
+                int hbase = 0;
+                if (lane == 0) {
+                    obase = atomicAdd(&P.st->out_count, (unsigned)nl);
+                    hbase = atomicAdd(&sNHoles, nl);
                 }
-                S.cell[slot] = -1;
-                int hpos = atomicAdd(&sNHoles, 1);
-                if (hpos < kHoleMax) sHoles[hpos] = j;
-                else bad |= ST_HOLES;
+                obase = __shfl_sync(FULL, obase, 0);
+                hbase = __shfl_sync(FULL, hbase, 0);
+                if (leave) {
+                    const unsigned e = obase + rank;
+                    if (e < P.out_cap) {
+                        OutMixed o;
+                        o.ox = xe[0]; o.oy = xe[1]; o.oz = xe[2]; o.px = pu; o.py = pv; o.pz = pw;
+                        o.cell = newcell;
+                        o.species = s;
+                        outbox[e] = o;
+                        moved++;
+                    } else {
+                        bad |= ST_OUTBOX;
+                    }
+                    S.cell[slot] = -1;
+                    const int hpos = hbase + rank;
+                    if (hpos < kHoleMax) sHoles[hpos] = j;
+                    else bad |= ST_HOLES;
+                }
             }
         }
-        flush_groups(wacc + (gbuf ^ 1) * (kGroups * kSlots), pend_lead, pend_n0, pend_sh);
         __syncwarp();
-        drain(qn);
-        if (unsorted) atomicAdd(&P.st->unsorted[s], (unsigned long long)unsorted);
+        drain_range(0, qn);
+        // the species' largest contribution bound, for the next push's quantum
+        lbmax = __uint_as_float(__reduce_max_sync(FULL, __float_as_uint(lbmax)));
+        if (lane == 0 && lbmax > 0.f) atomicMax(&sLbMax, __float_as_uint(lbmax));
         __syncthreads();
-        const int L = sNHoles;
-        if (L > 0 && L <= kHoleMax) {
-            const int newcount = count - L;
-            for (int r = threadIdx.x; r < L; r += blockDim.x) {
+        if (threadIdx.x == 0 && P.lb_cur && sLbMax) {
+            atomicMax(&P.lb_cur[s], sLbMax);
+            sLbMax = 0u;
+        }
+        // int32 currents of the species -> exact 64-bit tile J; clear them
+        for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
+            long long sum = 0;
+#pragma unroll
+            for (int c = 0; c < kJCopies; c++) {
+                sum += sJw[c * 3 * nn + idx];
+                sJw[c * 3 * nn + idx] = 0;
+            }
+            if (sum) sJ[idx] += (unsigned long long)rescale(sum, sh);
+        }
+        const int nh = sNHoles;
+        if (nh > 0 && nh <= kHoleMax) {
+            const int newcount = count - nh;
+            for (int r = threadIdx.x; r < nh; r += blockDim.x) {
                 int h = sHoles[r];
                 if (h < newcount) sFront[atomicAdd(&sNFront, 1)] = h;
             }
             __syncthreads();
-            for (int r = threadIdx.x; r < L; r += blockDim.x) {
+            for (int r = threadIdx.x; r < nh; r += blockDim.x) {
                 int src = start + newcount + r;
                 if (S.cell[src] >= 0) {
                     int mv = atomicAdd(&sNMove, 1);
@@ -587,7 +664,34 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(StepParams P) {
     if (moved) atomicAdd(&P.st->moved, moved);
 }
 
+// Contribution bound of a species from its current momenta, for the first
+// push after a load: 1.0834 max over particles and axes of |w_a| (tau/h_a)
+// |p_a| / gamma (the bound of a full step at the current velocity), as float
+// bits into *out (atomicMax)
+__global__ void k_contribution_bound(SpeciesView S, int n, float wx, float wy, float wz, float ctx, float cty,
+                                     float ctz, unsigned *out) {
+    float m = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (S.cell[i] < 0) continue;
+        const float pu = S.fx[i], pv = S.fy[i], pw = S.fz[i];
+        const float ig = rsqrtf(pu * pu + pv * pv + pw * pw + 1.f);
+        const float b = fmaxf(fabsf(wx) * ctx * fabsf(pu), fmaxf(fabsf(wy) * cty * fabsf(pv), fabsf(wz) * ctz * fabsf(pw)));
+        m = fmaxf(m, 1.0834f * b * ig);
+    }
+    m = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m)));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));
+}
+
 }  // namespace
+
+cudaError_t contribution_bound_mixed(const Grid &g, const SpeciesView &S, int64_t cap, unsigned *out, cudaStream_t s) {
+    if (cap <= 0) return cudaSuccess;
+    const float ctx = (float)(g.tau / g.hx), cty = (float)(g.tau / g.hy), ctz = (float)(g.tau / g.hz);
+    const float wx = (float)(S.m * g.hx / g.tau), wy = (float)(S.m * g.hy / g.tau), wz = (float)(S.m * g.hz / g.tau);
+    const int blocks = (int)std::min<int64_t>((cap + 255) / 256, 148 * 8);
+    k_contribution_bound<<<blocks, 256, 0, s>>>(S, (int)cap, wx, wy, wz, ctx, cty, ctz, out);
+    return cudaGetLastError();
+}
 
 constexpr int kPlaneThreads = 256;
 static inline dim3 plane_grid(const Grid &g) {
@@ -605,10 +709,43 @@ void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], dou
                                                      cy, cz, g.tau);
 }
 
-size_t push_smem_mixed(const Grid &g) {
-    size_t nn = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2);
-    return 6 * nn * sizeof(float4) + 3 * nn * sizeof(unsigned long long) + kHoleMax * sizeof(int);
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
 }
+
+cudaError_t encode_field_maps(const Grid &g, float *const E[3], float *const H[3], MixedMaps *maps) {
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return cudaErrorNotSupported;
+    // {z, y, x}: z rows of pitch pz floats (a multiple of 4: 16-byte strides);
+    // box = tile + halo, z rounded up to whole 16-byte units; the tile's first
+    // z node k0 is a multiple of tz (a multiple of 4), so every box starts on
+    // a 16-byte boundary
+    const cuuint64_t dims[3] = {(cuuint64_t)g.NZ, (cuuint64_t)g.NY, (cuuint64_t)g.NX};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.pz * sizeof(float), (cuuint64_t)g.pz * g.NY * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)(g.tz + 4), (cuuint32_t)(g.ty + 3), (cuuint32_t)(g.tx + 2)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (g.tz % 4 != 0 || box[0] > 256 || box[1] > 256 || box[2] > 256) return cudaErrorInvalidValue;
+    float *const src[6] = {E[0], E[1], E[2], H[0], H[1], H[2]};
+    for (int f = 0; f < 6; f++) {
+        CUresult r = encode(&maps->m[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)src[f], dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
+size_t push_smem_mixed(const Grid &g) { return mixed_smem(g.tx, g.ty, g.tz).total; }
 
 size_t push_smem_total_mixed(const Grid &g) {
     cudaFuncAttributes a;
@@ -616,11 +753,11 @@ size_t push_smem_total_mixed(const Grid &g) {
     return push_smem_mixed(g) + a.sharedSizeBytes;
 }
 
-cudaError_t launch_push_mixed(const StepParams &p, cudaStream_t s) {
+cudaError_t launch_push_mixed(const StepParams &p, const MixedMaps &maps, cudaStream_t s) {
     size_t smem = push_smem_mixed(p.g);
     cudaError_t e = cudaFuncSetAttribute(k_push_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_push_mixed<<<p.g.ntiles, kMixedThreads, smem, s>>>(p);
+    k_push_mixed<<<p.g.ntiles, kMixedThreads, smem, s>>>(maps, p);
     return cudaGetLastError();
 }
 

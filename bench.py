@@ -202,13 +202,7 @@ def run_ours(args, dist):
     import torch
 
     pkg = importlib.import_module("0buf_b200")
-    cfg = dict(pkg.configs.CONFIGS[args.config])
-    if args.cells:
-        cfg["cells"] = tuple(int(c) for c in args.cells.split(","))
-        args.config = "custom"
-    if args.ppc:
-        cfg["ppc"] = args.ppc
-        args.config = "custom"
+    cfg = workload_cfg(args, pkg.configs)
     form = args.form or cfg["precision"]
     dev = dist.local
     torch.cuda.set_device(dev)
@@ -257,12 +251,8 @@ def run_ours(args, dist):
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
         "ms_per_step": round(t_max / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if form == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {cells[0]}x{cells[1]}x{cells[2]} cells, {cfg['ppc']} particles/cell/"
-                               f"species x 3 species = {int(n_total / dist.world):,} particles per GPU, "
-                               f"{'FP32 mixed form (FP64 global J)' if form == 'fp32' else 'FP64 plain form'}",
-                   "cells": list(cells), "ppc": cfg["ppc"], "species": 3, "form": form, "tau": cfg["tau"],
-                   "h": cfg["h"], "parallelism": f"replicas x{dist.world}",
-                   "l2": f"inputs larger than L2 ({layout['bytes_per_particle'] * n_local / 1e9:.1f} GB of particles)"},
+        "form": "FP32 mixed form (FP64 global J)" if form == "fp32" else "FP64 plain form",
+        "config": workload_config(args, cfg, int(n_total / dist.world), dist.world),
         "roofline": roofline,
         "yee": yee,
         "phases_ms": {k: round(statistics.mean(v), 4) for k, v in phases.items()},
@@ -305,7 +295,7 @@ def run_ours(args, dist):
     if dist.world == 1 and args.stress_adjoint:
         out["adjoint_stress"] = run_adjoint_stress(args, pkg, dev)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(args)
+        out["cpu_baseline"] = cpu_baseline(args, cfg)
     return out
 
 
@@ -653,6 +643,15 @@ def run_e2e(args, dist, pkg, cfg, form, torch, n_local):
 
 
 # ------------------------------------------------------- CPU baselines
+# The reference's CPU path at the workload's density, on a periodic sub-box of
+# 64x32x32 cells (1/128 of the 512x128x128 workload: 6.3M particles, 0.65 GB of
+# the reference's 104-byte particles, well above the host caches).  Its
+# containers (one 5000-particle array per cell, cell.h:55, 254) cannot hold the
+# full workload.  Per-particle work is that of the full box: same species,
+# density, dt and h, periodic.
+REF_SAMPLE_CELLS = (64, 32, 32)
+
+
 def cpu_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -660,81 +659,147 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
-def cpu_sim(kind_pref="reference"):
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    oracle = importlib.import_module("oracle")
-    if kind_pref == "reference" and oracle.RefSim.available():
-        return oracle.RefSim, "reference"
-    return oracle.OracleSim, "port"
+    return importlib.import_module("oracle")
 
 
-def cpu_run(seconds: float, min_steps: int, max_steps: int, threads: int, kind_pref="reference"):
-    """The reference CPU path at its own case (32x4x4 cells, 32 ppc x 3 species)."""
-    import numpy as np
-    pkg = importlib.import_module("0buf_b200")
-    Sim, kind = cpu_sim(kind_pref)
-    cfg = pkg.configs.CONFIGS["c0"]
-    cells, h, tau, ppc = cfg["cells"], cfg["h"], cfg["tau"], cfg["ppc"]
+def species_of(cfg):
+    """Species table rows (q_m, m, sort) and generator arguments of a
+    configuration (plain data only: no product library is loaded)."""
+    configs = importlib.import_module("0buf_b200.configs")
+    sp = cfg.get("species") or configs.SPECIES_BEAM_PLASMA
+    return configs.species_table(cfg["ppc"], sp), sp
+
+
+def cpu_sim(cfg, cells, threads, kind):
+    """A CPU simulation of `cells` at the configuration's density: the
+    reference's own functions (kind "reference", oracle/_ref) or the C
+    restatement (kind "port"), inputs from the oracle's restated generator."""
+    oracle = _oracle()
+    table, sp = species_of(cfg)
+    if any("profile" in s for s in sp):
+        raise ValueError("CPU baselines cover the uniform configurations")
+    h, tau, ppc = cfg["h"], cfg["tau"], cfg["ppc"]
     box = tuple(c * h for c in cells)
-    sim = Sim(cells, box, tau, threads=threads)
-    table = pkg.configs.species_table(ppc)
-    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
-        arrs = pkg.host_species(cells, box, i, ppc, s["drift"], s["vth"], 0)
-        sim.add_particles(s["sort"], *arrs, table[i][1], s["q_m"])
+    if kind == "reference":
+        sim = oracle.RefSim(cells, box, tau, threads=threads)
+        for i, s in enumerate(sp):
+            arrs = oracle.gen_species(cells, box, i, ppc, s["drift"], s["vth"], i, threads=threads)
+            sim.add_particles(s["sort"], *arrs, table[i][1], s["q_m"])
+    else:
+        sim = oracle.OracleSim(cells, box, tau, threads=threads)
+        for i, s in enumerate(sp):
+            sim.init_species(s["sort"], i, ppc, s["drift"], s["vth"], i, table[i][1], s["q_m"])
+    return sim
+
+
+def cpu_time(cfg, cells, threads, kind, seconds, min_steps=1, max_steps=100000, warm=True):
+    """Full PIC steps of the CPU path on `cells` with `threads` threads until
+    `seconds` have passed (at least min_steps), after one untimed step unless
+    warm is False.  The inputs are built with all host threads."""
+    sim = cpu_sim(cfg, cells, cpu_threads(), kind)
+    sim.set_threads(threads)
     n = sim.num_particles()
-    sim.step()  # warm
+    if warm:
+        assert sim.step() == 0
     steps, t0 = 0, time.perf_counter()
     while steps < max_steps and (steps < min_steps or time.perf_counter() - t0 < seconds):
         assert sim.step() == 0
         steps += 1
     dt = time.perf_counter() - t0
     sim.close()
-    return dict(value=round(n * steps / dt, 1), unit=UNIT, cores=threads, kind=kind,
-                sample=f"{steps} steps of the 32x4x4-cell case ({n} particles) with {threads} threads, "
-                       f"{dt:.1f} s; {'reference functions compiled for the host (oracle/_ref)' if kind == 'reference' else 'C restatement (oracle/cpu_pic.c)'}",
-                np=int(np.int64(n)))
+    return {"value": round(n * steps / dt, 1), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{steps} steps of {cells[0]}x{cells[1]}x{cells[2]} cells ({n:,} particles), "
+                      f"{threads} thread(s), {dt:.1f} s", "particles": n}
 
 
-def cpu_baseline(args):
-    return cpu_run(args.cpu_seconds, 5, 100000, cpu_threads())
+def ref_kind() -> str:
+    return "reference" if _oracle().RefSim.available() else "port"
+
+
+def cpu_baseline(args, cfg):
+    """The reference CPU path on the box's host cores, rank 0 at N=1: the
+    headline figure is the reference's own functions (oracle/_ref) on all
+    cores on the workload's 64x32x32-cell sample; `configs` adds the C
+    restatement (oracle/cpu_pic.c, bit-identical to the reference's
+    functions) at the configurations c0, c3 (one thread and all cores) and
+    c1 (all cores; one thread times one step when host RAM and time allow)."""
+    import psutil
+    configs = importlib.import_module("0buf_b200.configs")
+    thr = cpu_threads()
+    kind = ref_kind()
+    head = cpu_time(cfg, REF_SAMPLE_CELLS, thr, kind, args.cpu_seconds)
+    head["sample"] += (f" -- a periodic sub-box of the {'x'.join(map(str, cfg['cells']))}-cell workload at its "
+                       f"density; {'reference functions compiled for the host (oracle/_ref)' if kind == 'reference' else 'C restatement (oracle/cpu_pic.c)'}")
+    out = dict(head)
+    out["configs"] = {}
+    runs = [("c0", "reference" if kind == "reference" else "port", thr, 4.0, True),
+            ("c3", "port", 1, 0.0, False), ("c3", "port", thr, 2.0, True), ("c1", "port", thr, 0.0, True)]
+    for name, k, t, secs, warm in runs:
+        c = configs.CONFIGS[name]
+        n = int(c["cells"][0] * c["cells"][1] * c["cells"][2]) * c["ppc"] * 3
+        if psutil.virtual_memory().available < 200 * n:  # ~96 B per port particle plus tiles, with margin
+            out["configs"][f"{name}_{t}t"] = {"value": None, "note": "host RAM"}
+            continue
+        r = cpu_time(c, c["cells"], t, k, secs, warm=warm)
+        out["configs"][f"{name}_{t}t"] = r
+    out["configs"]["c1_1t"] = {"value": None, "note": "not run by default: one single-thread step of the 201M "
+                                                      "particles takes over a minute; c3_1t is the single-thread rate"}
+    return out
 
 
 def run_reference(args):
-    """--impl reference: the reference's own CPU implementation, rank 0 only."""
+    """--impl reference: the reference's own CPU implementation, rank 0 only,
+    on the same workload and metric as our arm: each benchmark step is one
+    PIC step of the workload's 64x32x32-cell periodic sample (REF_SAMPLE_CELLS)
+    on all host cores."""
+    configs = importlib.import_module("0buf_b200.configs")
+    cfg = workload_cfg(args, configs)
     threads = cpu_threads()
-    pkg = importlib.import_module("0buf_b200")
-    Sim, kind = cpu_sim("reference")
-    cfg = pkg.configs.CONFIGS["c0"]
-    cells, h, tau, ppc = cfg["cells"], cfg["h"], cfg["tau"], cfg["ppc"]
-    box = tuple(c * h for c in cells)
-    sim = Sim(cells, box, tau, threads=threads)
-    table = pkg.configs.species_table(ppc)
-    for i, s in enumerate(pkg.configs.SPECIES_BEAM_PLASMA):
-        arrs = pkg.host_species(cells, box, i, ppc, s["drift"], s["vth"], 0)
-        sim.add_particles(s["sort"], *arrs, table[i][1], s["q_m"])
+    kind = ref_kind()
+    sim = cpu_sim(cfg, REF_SAMPLE_CELLS, threads, kind)
     n = sim.num_particles()
     for _ in range(args.warmup):
         assert sim.step() == 0
-    # each benchmark step: a bounded sample of PIC steps of the case
-    inner = max(1, args.reference_inner)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        for _ in range(inner):
-            assert sim.step() == 0
+        assert sim.step() == 0
     dt = time.perf_counter() - t0
     sim.close()
-    value = n * args.steps * inner / dt
-    sample = (f"{args.steps} x {inner} steps of the 32x4x4-cell case ({n} particles), {threads} threads; "
+    value = n * args.steps / dt
+    n_full = int(cfg["cells"][0] * cfg["cells"][1] * cfg["cells"][2]) * cfg["ppc"] * 3
+    sample = (f"{args.steps} steps (after {args.warmup} warm-up) of a {'x'.join(map(str, REF_SAMPLE_CELLS))}-cell periodic "
+              f"sub-box of the workload at its density ({n:,} particles), {threads} threads; "
               f"{'reference functions compiled for the host (oracle/_ref)' if kind == 'reference' else 'C restatement of the reference (oracle/cpu_pic.c)'}")
     return {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "c0: 32x4x4 cells, 32 particles/cell/species x 3 species (the reference's "
-                                   "CPU-runnable case; its per-cell 5000-slot containers cannot hold the GPU configs)",
-                       "cells": list(cells), "ppc": ppc},
+            "form": "reference CPU path (FP64)",
+            "config": workload_config(args, cfg, n_full, 1),
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def workload_cfg(args, configs):
+    cfg = dict(configs.CONFIGS[args.config])
+    if args.cells:
+        cfg["cells"] = tuple(int(c) for c in args.cells.split(","))
+    if args.ppc:
+        cfg["ppc"] = args.ppc
+    return cfg
+
+
+def workload_config(args, cfg, n_per_gpu, world):
+    """The `config` object of both arms: the workload, nothing of the arm."""
+    cells = cfg["cells"]
+    name = args.config if not (args.cells or args.ppc) else "custom"
+    return {"workload": f"{name}: {cells[0]}x{cells[1]}x{cells[2]} cells, {cfg['ppc']} particles/cell/species x 3 "
+                        f"species = {n_per_gpu:,} particles per GPU",
+            "cells": list(cells), "ppc": cfg["ppc"], "species": 3, "tau": cfg["tau"], "h": cfg["h"],
+            "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 ({28 * n_per_gpu / 1e9:.1f} GB of FP32-form particles; no flush needed)"}
 
 
 def main():

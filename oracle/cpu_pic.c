@@ -709,3 +709,115 @@ long op_get_particles(void *h, double *out, int *cell, int *sort, int *direction
     }
     return j;
 }
+
+/* ------------------------------------------------ seeded initial particles */
+/* Restatement of the library's counter-based generator of the benchmark
+ * configurations' particles (0buf_b200/csrc/pic_rng.cuh, used by
+ * pic_init_species_host and the device generator): per interior cell
+ * (i, l, k) in i, l, k order, dense index c = (i*ny + l)*nz + k, ppc particles
+ * at uniform in-cell offsets o in [1e-6, 1 - 1e-6] and momenta
+ * drift + vth * N(0,1) per axis (Box-Muller).  Keys: SplitMix64's finaliser
+ * (Steele, Lea, Flood 2014) chained over (seed, species, cell, slot, stream).
+ * tests/test_oracle_generator.py checks it bit for bit against
+ * pic_init_species_host.  The reference has no such generator (its loader is
+ * the quiet start of maxwell.cu); this one exists so the CPU baselines and the
+ * reference arm build their inputs without the product library. */
+static inline uint64_t og_mix(uint64_t z) {
+    z ^= z >> 30;
+    z *= 0xBF58476D1CE4E5B9ull;
+    z ^= z >> 27;
+    z *= 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return z;
+}
+static inline uint64_t og_key(uint64_t seed, int species, int64_t cell, int slot, int stream) {
+    uint64_t h = og_mix(seed + 0x9E3779B97F4A7C15ull);
+    h = og_mix(h ^ ((uint64_t)(uint32_t)species * 0xD6E8FEB86659FD93ull));
+    h = og_mix(h ^ ((uint64_t)cell * 0xA0761D6478BD642Full));
+    h = og_mix(h ^ ((uint64_t)(uint32_t)slot * 0xE7037ED1A0B428DBull));
+    h = og_mix(h ^ ((uint64_t)(uint32_t)stream * 0x8EBC6AF09C88C6E3ull));
+    return h;
+}
+static inline double og_uniform(uint64_t seed, int species, int64_t cell, int slot, int stream) {
+    return (double)(og_key(seed, species, cell, slot, stream) >> 11) * (1.0 / 9007199254740992.0);
+}
+static inline double og_offset(uint64_t seed, int species, int64_t cell, int slot, int axis) {
+    return 1e-6 + og_uniform(seed, species, cell, slot, axis) * (1.0 - 2e-6);
+}
+static inline double og_normal(uint64_t seed, int species, int64_t cell, int slot, int axis) {
+    int pair = axis < 2 ? 0 : 1;
+    double u1 = 1.0 - og_uniform(seed, species, cell, slot, 8 + 2 * pair);
+    double u2 = og_uniform(seed, species, cell, slot, 9 + 2 * pair);
+    double r = sqrt(-2.0 * log(u1));
+    double a = 6.283185307179586 * u2;
+    return (axis == 1) ? r * sin(a) : r * cos(a);
+}
+/* one particle: slot s of dense cell c at (i, l, k); out = x y z px py pz */
+static void og_particle(double hx, double hy, double hz, int i, int l, int k, int64_t c, int s, int species,
+                        double dx, double dy, double dz, double vth, uint64_t seed, double out[6]) {
+    double ox = og_offset(seed, species, c, s, 0);
+    double oy = og_offset(seed, species, c, s, 1);
+    double oz = og_offset(seed, species, c, s, 2);
+    out[0] = (double)i * hx + ox * hx;
+    out[1] = (double)l * hy + oy * hy;
+    out[2] = (double)k * hz + oz * hz;
+    if (vth != 0.0) {
+        out[3] = dx + vth * og_normal(seed, species, c, s, 0);
+        out[4] = dy + vth * og_normal(seed, species, c, s, 1);
+        out[5] = dz + vth * og_normal(seed, species, c, s, 2);
+    } else {
+        out[3] = dx; out[4] = dy; out[5] = dz;
+    }
+}
+
+/* The generator into flat arrays (cell-major order), threads over cells. */
+int op_gen_species(int nx, int ny, int nz, double lx, double ly, double lz, int species, int ppc, double dx,
+                   double dy, double dz, double vth, uint64_t seed, int threads, double *x, double *y, double *z,
+                   double *px, double *py, double *pz) {
+    if (nx < 1 || ny < 1 || nz < 1 || ppc < 0) return -1;
+    double hx = lx / ((double)nx), hy = ly / ((double)ny), hz = lz / ((double)nz);
+    long ncell = (long)nx * ny * nz;
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(static)
+    for (long c = 0; c < ncell; c++) {
+        int i = (int)(c / ((long)ny * nz)), l = (int)((c / nz) % ny), k = (int)(c % nz);
+        for (int s = 0; s < ppc; s++) {
+            double o[6];
+            long q = c * ppc + s;
+            og_particle(hx, hy, hz, i, l, k, c, s, species, dx, dy, dz, vth, seed, o);
+            x[q] = o[0]; y[q] = o[1]; z[q] = o[2]; px[q] = o[3]; py[q] = o[4]; pz[q] = o[5];
+        }
+    }
+    return 0;
+}
+
+/* The generator straight into the simulation's cell lists, threads over
+ * cells: the same particles, in the same per-cell order, as op_gen_species
+ * followed by op_add_particles (each generated particle lies strictly inside
+ * its cell).  Returns the particles inserted. */
+long op_init_species(void *h, int sort, int species, int ppc, double dx, double dy, double dz, double vth,
+                     uint64_t seed, double m, double q_m) {
+    op_sim *s = (op_sim *)h;
+    long ncell = (long)s->Nx * s->Ny * s->Nz;
+    long inserted = 0;
+    int fail = 0;
+#pragma omp parallel for num_threads(s->threads) schedule(dynamic, 64) reduction(+ : inserted) reduction(| : fail)
+    for (long c = 0; c < ncell; c++) {
+        int i = (int)(c / ((long)s->Ny * s->Nz)), l = (int)((c / s->Nz) % s->Ny), k = (int)(c % s->Nz);
+        for (int q = 0; q < ppc; q++) {
+            double o[6];
+            og_particle(s->hx, s->hy, s->hz, i, l, k, c, q, species, dx, dy, dz, vth, seed, o);
+            /* getPointCell as op_add_particles */
+            int ci = (int)((o[0] - 0.0) / s->hx), cl = (int)((o[1] - 0.0) / s->hy), ck = (int)((o[2] - 0.0) / s->hz);
+            long cn = glob(s, ci, cl, ck);
+            if (cn != glob(s, i, l, k)) continue; /* never for offsets inside [1e-6, 1 - 1e-6] */
+            op_particle p;
+            p.x = o[0]; p.y = o[1]; p.z = o[2]; p.pu = o[3]; p.pv = o[4]; p.pw = o[5];
+            p.m = m; p.q_m = q_m; p.x1 = p.y1 = p.z1 = 0.0; p.sort = sort; p.direction = 13;
+            cgeo g = geo(s, cn);
+            if (!in_cell(s, &g, &p)) continue;
+            if (cell_append(&s->cells[cn], &p)) { fail = 1; break; }
+            inserted++;
+        }
+    }
+    return fail ? -1 : inserted;
+}

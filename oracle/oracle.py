@@ -163,7 +163,22 @@ class OracleSim(_Sim):
             lib.op_energies.restype = C.c_int
             lib.op_status.argtypes = [C.c_void_p]
             lib.op_status.restype = C.c_int
+            lib.op_gen_species.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [C.c_int, C.c_int] + \
+                [C.c_double] * 4 + [C.c_uint64, C.c_int] + [D] * 6
+            lib.op_gen_species.restype = C.c_int
+            lib.op_init_species.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_double] * 4 + \
+                [C.c_uint64, C.c_double, C.c_double]
+            lib.op_init_species.restype = C.c_long
         return cls._lib
+
+    def init_species(self, sort, species_index, ppc, drift, vth, seed, m, q_m) -> int:
+        """The seeded generator (gen_species) straight into the cell lists, in
+        parallel over cells: the same state as add_particles of its arrays."""
+        n = int(self.L.op_init_species(self.h, int(sort), int(species_index), int(ppc),
+                                       *[float(d) for d in drift], float(vth), int(seed), float(m), float(q_m)))
+        if n < 0:
+            raise MemoryError("op_init_species")
+        return n
 
     def set_threads(self, n):
         self.L.op_set_threads(self.h, int(n))
@@ -192,6 +207,21 @@ class RefSim(_Sim):
     @classmethod
     def available(cls) -> bool:
         return os.path.exists(cls.libpath)
+
+
+def gen_species(cells, lengths, species_index, ppc, drift=(0.0, 0.0, 0.0), vth=0.0, seed=0, threads=1):
+    """The library's seeded initial particles restated in C (op_gen_species):
+    x, y, z, px, py, pz arrays in cell-major order, bit-identical to the
+    library's pic_init_species_host."""
+    lib = OracleSim.lib()
+    n = int(np.prod(cells)) * int(ppc)
+    arrs = [np.zeros(n) for _ in range(6)]
+    rc = lib.op_gen_species(*[int(c) for c in cells], *[float(v) for v in lengths], int(species_index), int(ppc),
+                            *[float(d) for d in drift], float(vth), int(seed), int(threads),
+                            *[a.ctypes.data_as(D) for a in arrs])
+    if rc != 0:
+        raise ValueError("op_gen_species")
+    return arrs
 
 
 # ---------------------------------------------------------------------------
