@@ -3,7 +3,9 @@
 Every translation unit is compiled by nvcc for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``).  The FP64 parity code (plain
 form, binning, C ABI) is compiled with ``-fmad=false`` so its arithmetic is the
-reference's separate IEEE multiplies and adds; the FP32 mixed form keeps FMA.
+reference's separate IEEE multiplies and adds; the FP32 mixed form keeps FMA
+and flushes FP32 subnormals (``-ftz=true``: no subnormal handling around the
+reciprocal square roots and divisions of its push).
 The CUDA runtime is linked statically so the ``.so`` is self-contained.
 
 Usage: ``python 0buf_b200/build.py [--force] [-j N]``.
@@ -33,7 +35,7 @@ UNITS = {
     "pic_common.cu": ["-fmad=false"],
     "pic_capi.cu": ["-fmad=false"],
     "pic_arch.cu": [],
-    "pic_mixed.cu": [],
+    "pic_mixed.cu": ["-ftz=true"],
     "pic_noalloc.cu": [],
     "pic_diag.cu": ["-fmad=false"],
     "pic_dump.cu": [],

@@ -110,6 +110,8 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
         int64_t pad = h->cfg.capacity_pad >= 0 ? h->cfg.capacity_pad : 64;
         int64_t cap = (int64_t)counts[t] + (int64_t)ceil(counts[t] * slack) + pad;
         if (pad > 0) cap = (cap + 31) / 32 * 32;
+        // the FP32 push reads and writes particles in 8-byte pairs: every tile starts on an even slot
+        if (h->mixed) cap = (cap + 1) / 2 * 2;
         // the plain form's two-word tile J stays exact up to kFxMaxTileSlots
         // particles in a tile over all species
         if (!h->mixed && cap > kFxMaxTileSlots / h->cfg.nspecies)

@@ -61,12 +61,17 @@ __global__ void k_e_update_mixed(Grid g, float *Ex, float *Ey, float *Ez, const 
 // 128-bit shared loads (the same products and sums, in the same order, as
 // the 8 scalar taps).  Q points at the stencil's lower node; the upper x node
 // is SYZ quads further; sx, sy, sz weight the lower node of each axis.
-__device__ __forceinline__ float interp_quad(const float4 *__restrict__ Q, int SYZ, float sx, float sy, float sz) {
+// The trilinear weights are applied with packed FP32x2 arithmetic
+// (fma.rn.f32x2): x first on the (z lower, z upper) pairs of the lower and
+// upper y rows, then y on the pair, then z.  w = (s, 1 - s) per axis, s
+// weighting the lower node.
+__device__ __forceinline__ float interp_quad2(const float4 *__restrict__ Q, int SYZ, float2 wx, float2 wy, float2 wz) {
     const float4 A = Q[0], B = Q[SYZ];
-    const float sx1 = 1.f - sx, sy1 = 1.f - sy, sz1 = 1.f - sz;
-    float t1 = sx * (sy * (sz * A.x + sz1 * A.y) + sy1 * (sz * A.z + sz1 * A.w));
-    float t2 = sx1 * (sy * (sz * B.x + sz1 * B.y) + sy1 * (sz * B.z + sz1 * B.w));
-    return t1 + t2;
+    const float2 ax = make_float2(wx.x, wx.x), bx = make_float2(wx.y, wx.y);
+    const float2 r0 = __ffma2_rn(bx, make_float2(B.x, B.y), __fmul2_rn(ax, make_float2(A.x, A.y)));
+    const float2 r1 = __ffma2_rn(bx, make_float2(B.z, B.w), __fmul2_rn(ax, make_float2(A.z, A.w)));
+    const float2 r = __ffma2_rn(make_float2(wy.y, wy.y), r1, __fmul2_rn(make_float2(wy.x, wy.x), r0));
+    return fmaf(wz.y, r.y, wz.x * r.x);
 }
 
 // pqr (cell.h:1511-1693) in cell units: the 12 contributions of the segment
@@ -100,6 +105,40 @@ __device__ __forceinline__ void pqr_mixed(const int iv[3], const float xs[3], co
     v[11] = sw * (dx * dy + s3);
 }
 
+// pqr_mixed with the centre planes given as float offsets c_a = iv_a - 2.5
+// (each -1/2 or +1/2: no integer-to-float conversions) and packed FP32x2
+// arithmetic, each contribution rounded to an
+// integer number of quanta: w[q] = round(v[q] / q_s), via the FMA magic
+// number 1.5 * 2^23 (exact for |v / q_s| < 2^22).  inv_qs = 1 / q_s.
+__device__ __forceinline__ void pqr_quant(const float cc[3], const float xs[3], const float xe[3], float wx, float wy,
+                                          float wz, float inv_qs, int w[12]) {
+    const float dx = 0.5f * (xs[0] + xe[0]) - cc[0];
+    const float dy = 0.5f * (xs[1] + xe[1]) - cc[1];
+    const float dz = 0.5f * (xs[2] + xe[2]) - cc[2];
+    const float su = xe[0] - xs[0], sv = xe[1] - xs[1], sw = xe[2] - xs[2];
+    const float r12 = 1.f / 12.f;
+    const float s1 = sv * sw * r12, s2 = su * sw * r12, s3 = su * sv * r12;
+    // per component: (lower, upper) weights of the two transverse axes
+    const float2 DZ = make_float2(1.f - dz, dz), DY = make_float2(1.f - dy, dy);
+    const float2 M = make_float2(12582912.0f, 12582912.0f);
+    const float ax = su * wx * inv_qs, ay = sv * wy * inv_qs, az = sw * wz * inv_qs;
+    float2 r[6];
+    // Jx: su (dy1 dz1 + s1, dy1 dz - s1, dy dz1 - s1, dy dz + s1)
+    r[0] = __ffma2_rn(make_float2(ax, ax), __ffma2_rn(make_float2(DY.x, DY.x), DZ, make_float2(s1, -s1)), M);
+    r[1] = __ffma2_rn(make_float2(ax, ax), __ffma2_rn(make_float2(DY.y, DY.y), DZ, make_float2(-s1, s1)), M);
+    // Jy: sv (dx1 dz1 + s2, dx1 dz - s2, dx dz1 - s2, dx dz + s2)
+    r[2] = __ffma2_rn(make_float2(ay, ay), __ffma2_rn(make_float2(1.f - dx, 1.f - dx), DZ, make_float2(s2, -s2)), M);
+    r[3] = __ffma2_rn(make_float2(ay, ay), __ffma2_rn(make_float2(dx, dx), DZ, make_float2(-s2, s2)), M);
+    // Jz: sw (dx1 dy1 + s3, dx1 dy - s3, dx dy1 - s3, dx dy + s3)
+    r[4] = __ffma2_rn(make_float2(az, az), __ffma2_rn(make_float2(1.f - dx, 1.f - dx), DY, make_float2(s3, -s3)), M);
+    r[5] = __ffma2_rn(make_float2(az, az), __ffma2_rn(make_float2(dx, dx), DY, make_float2(-s3, s3)), M);
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        w[2 * q] = __float_as_int(r[q].x) - 0x4B400000;
+        w[2 * q + 1] = __float_as_int(r[q].y) - 0x4B400000;
+    }
+}
+
 // tile-local J index of contribution j of a segment whose base node is nb
 __device__ __forceinline__ int contrib_node(int j, int nb, int nn, int SY, int SZ) {
     int comp = j >> 2, r = j & 3;
@@ -118,22 +157,21 @@ __device__ __forceinline__ int contrib_node(int j, int nb, int nn, int SY, int S
 // over the crossing axes c -- the reference's formula for one crossing axis
 // (cases 1, 2, 4: a ratio) and for two (cases 3, 5, 6: the point nearest to
 // both planes); with three crossing axes x2 is the centre.  Without a crossing
-// x2 = xe: the second segment then has length 0 and adds nothing.
-__device__ __forceinline__ void split_point(const int i1[3], const int i2[3], const float xs[3], const float xe[3],
-                                            float x2[3]) {
+// x2 = xe: the second segment then has length 0 and adds nothing.  c[a]: the
+// centre index changes along axis a.
+__device__ __forceinline__ void split_point(const bool c[3], const float xs[3], const float xe[3], float x2[3]) {
     float num = 0.f, den = 0.f;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        float dl = xe[d] - xs[d];
-        bool c = i1[d] != i2[d];
-        num += c ? (0.5f - xs[d]) * dl : 0.f;
-        den += c ? dl * dl : 0.f;
+        const float dl = xe[d] - xs[d];
+        num += c[d] ? (0.5f - xs[d]) * dl : 0.f;
+        den += c[d] ? dl * dl : 0.f;
     }
-    const bool any = den > 0.f;
-    const float sr = any ? __fdividef(num, den) : 1.f;
+    const float sr = den > 0.f ? __fdividef(num, den) : 1.f;
 #pragma unroll
-    for (int d = 0; d < 3; d++) x2[d] = (i1[d] != i2[d]) ? 0.5f : xs[d] + (xe[d] - xs[d]) * sr;
+    for (int d = 0; d < 3; d++) x2[d] = c[d] ? 0.5f : xs[d] + (xe[d] - xs[d]) * sr;
 }
+
 
 // 2^e as float by exponent bits (no library call, no branch);
 // valid for -126 < e < 128
@@ -262,6 +300,9 @@ __host__ __device__ inline MixedSmem mixed_smem(int tx, int ty, int tz) {
 }
 
 #define PIC_MIXED_BOUNDS __launch_bounds__(kMixedThreads, PIC_MIXED_MIN_BLOCKS)
+// TX, TY, TZ: the tile's cells per axis when fixed at compile time (shared-
+// memory offsets become immediates), 0 to take them from the grid
+template <int TX, int TY, int TZ>
 __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps maps, StepParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long sBar;
@@ -274,17 +315,18 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     // queued segments: {stencil origin node, class bits, start x,y,z, end x,y,z}
     __shared__ float4 sQueue[kMixedWarps][kQueue][2];
     const Grid &g = P.g;
+    const int tx = TX ? TX : g.tx, ty = TY ? TY : g.ty, tz = TZ ? TZ : g.tz;
     const int t = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     const unsigned lt = (1u << lane) - 1;
     const int tk = t % g.ntz, tl = (t / g.ntz) % g.nty, ti = t / (g.ntz * g.nty);
-    const int i0 = ti * g.tx, l0 = tl * g.ty, k0 = tk * g.tz;
-    const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
+    const int i0 = ti * tx, l0 = tl * ty, k0 = tk * tz;
+    const int SX = tx + 2, SY = ty + 2, SZ = tz + 2;
     const int SYZ = SY * SZ;
     const int nn = SX * SYZ;
-    const int BY = g.ty + 3, BZ = g.tz + 4;
-    const MixedSmem L = mixed_smem(g.tx, g.ty, g.tz);
+    const int BY = ty + 3, BZ = tz + 4;
+    const MixedSmem L = mixed_smem(tx, ty, tz);
     float4 *sF = (float4 *)(smem_raw + L.quads);  // Ex Ey Ez Hx Hy Hz as yz-quads
     unsigned long long *sJ = (unsigned long long *)(smem_raw + L.tilej);
     int *sJw = (int *)(smem_raw + L.jw);
@@ -313,7 +355,7 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned comp_bytes = (unsigned)((size_t)(g.tx + 2) * BY * BZ * sizeof(float));
+        const unsigned comp_bytes = (unsigned)((size_t)SX * BY * BZ * sizeof(float));
         mbar_arrive_expect_tx(&sBar, 6 * comp_bytes);
 #pragma unroll
         for (int f = 0; f < 6; f++)
@@ -344,6 +386,11 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     float4(*queue)[2] = sQueue[warp];
 
     const float ctx = (float)(g.tau / g.hx), cty = (float)(g.tau / g.hy), ctz = (float)(g.tau / g.hz);
+    // packed cell index strides of x and y
+    const int cstr_x = 1 << (g.by + g.bz), cstr_y = 1 << g.bz;
+    // the tile's cells per axis inside the grid (the last tile of an axis can be
+    // cut short): a step past them leaves the tile, periodically wrapped or not
+    const int txe = min(tx, g.nx - i0), tye = min(ty, g.ny - l0), tze = min(tz, g.nz - k0);
     unsigned bad = 0;
     double kin = 0.0;
     unsigned long long moved = 0;
@@ -412,7 +459,8 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             int i = i0, l = l0, k = k0;
             if (active) {
                 g.cell_ijk(cur.cell, i, l, k);
-                if (i - i0 < 0 || i - i0 >= g.tx || l - l0 < 0 || l - l0 >= g.ty || k - k0 < 0 || k - k0 >= g.tz) {
+                if ((unsigned)(i - i0) >= (unsigned)tx || (unsigned)(l - l0) >= (unsigned)ty ||
+                    (unsigned)(k - k0) >= (unsigned)tz) {
                     bad |= ST_BADCELL;  // a bin entry outside its tile: never index the tile with it
                     active = false;
                     i = i0; l = l0; k = k0;
@@ -428,17 +476,22 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             // ---- GetField (cell.h:1257-1290) in cell units: getCellNumber = 2,
             // getCellNumberCenter = 2 + (offset >= 1/2), weights s1 = 1-o, s2 = 1/2-o (+1)
             const int cx = xs[0] >= 0.5f, cy = xs[1] >= 0.5f, cz = xs[2] >= 0.5f;
-            const int i1x = 2 + cx, i1y = 2 + cy, i1z = 2 + cz;
-            const float s1 = 1.f - xs[0], s2 = (cx ? 1.5f : 0.5f) - xs[0];
-            const float s3 = 1.f - xs[1], s4 = (cy ? 1.5f : 0.5f) - xs[1];
-            const float s5 = 1.f - xs[2], s6 = (cz ? 1.5f : 0.5f) - xs[2];
+            // centre offsets iv - 2.5 of the particle's cell-centre cell (+-1/2)
+            const float cc[3] = {cx ? 0.5f : -0.5f, cy ? 0.5f : -0.5f, cz ? 0.5f : -0.5f};
+            // (lower-node weight, upper-node weight) per axis: node-centred n, cell-centred c
+            const float2 nx = make_float2(1.f - xs[0], xs[0]), ny = make_float2(1.f - xs[1], xs[1]),
+                         nz = make_float2(1.f - xs[2], xs[2]);
+            // cell-centred lower weight s2 = (1/2 or 3/2) - o = 1 + c - o (getCellNumberCenter)
+            const float2 kx = make_float2(1.f + cc[0] - xs[0], xs[0] - cc[0]),
+                         ky = make_float2(1.f + cc[1] - xs[1], xs[1] - cc[1]),
+                         kz = make_float2(1.f + cc[2] - xs[2], xs[2] - cc[2]);
             const int ox = cx * SYZ, oy = cy * SZ, oz = cz;
-            float fEx = interp_quad(sF + lc + oy + oz, SYZ, s1, s4, s6);
-            float fEy = interp_quad(sF + nn + lc + ox + oz, SYZ, s2, s3, s6);
-            float fEz = interp_quad(sF + 2 * nn + lc + ox + oy, SYZ, s2, s4, s5);
-            float fHx = interp_quad(sF + 3 * nn + lc + ox, SYZ, s2, s3, s5);
-            float fHy = interp_quad(sF + 4 * nn + lc + oy, SYZ, s1, s4, s5);
-            float fHz = interp_quad(sF + 5 * nn + lc + oz, SYZ, s1, s3, s6);
+            float fEx = interp_quad2(sF + lc + oy + oz, SYZ, nx, ky, kz);
+            float fEy = interp_quad2(sF + nn + lc + ox + oz, SYZ, kx, ny, kz);
+            float fEz = interp_quad2(sF + 2 * nn + lc + ox + oy, SYZ, kx, ky, nz);
+            float fHx = interp_quad2(sF + 3 * nn + lc + ox, SYZ, kx, ny, nz);
+            float fHy = interp_quad2(sF + 4 * nn + lc + oy, SYZ, nx, ky, nz);
+            float fHz = interp_quad2(sF + 5 * nn + lc + oz, SYZ, nx, ny, kz);
 
             // ---- Particle::Move (particle.h:65-202), FP32
             pu += tau1 * fEx;
@@ -469,15 +522,21 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             float xe[3] = {xs[0] + ctx * (ig * pu), xs[1] + cty * (ig * pv), xs[2] + ctz * (ig * pw)};
 
             // ---- CurrentToMesh (cell.h:1306-1422) in cell units
-            // cell-centre index of the end point from the same exact float
-            // thresholds as i1 (x + 2.5 rounded in FP32 would put a point one
-            // ulp below a centre plane on the far side of it)
-            const int i1[3] = {i1x, i1y, i1z};
-            int i2[3];
+            // cell-centre class of the end point from the same exact float
+            // thresholds as the start's (x + 2.5 rounded in FP32 would put a
+            // point one ulp below a centre plane on the far side of it); the
+            // stencil holds -1/2 <= xe < 3/2 per axis (centre index 2 or 3)
+            bool ge[3], crs[3], inside = true;
 #pragma unroll
-            for (int d = 0; d < 3; d++) i2[d] = 2 + (xe[d] >= 0.5f) + (xe[d] >= 1.5f) - (xe[d] < -0.5f);
+            for (int d = 0; d < 3; d++) {
+                ge[d] = xe[d] >= 0.5f;
+                inside = inside && xe[d] >= -0.5f && xe[d] < 1.5f;
+            }
+            crs[0] = ge[0] != (bool)cx;
+            crs[1] = ge[1] != (bool)cy;
+            crs[2] = ge[2] != (bool)cz;
             bool dep = active && finite;
-            if (dep && (i2[0] < 2 || i2[0] > 3 || i2[1] < 2 || i2[1] > 3 || i2[2] < 2 || i2[2] > 3)) {
+            if (dep && !inside) {
                 bad |= ST_STENCIL;
                 dep = false;
             }
@@ -497,22 +556,19 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
                 run += add;
             }
             // the second zigzag segment exists only where a cell-centre plane is crossed
-            const bool cross = dep && (i2[0] != i1x || i2[1] != i1y || i2[2] != i1z);
+            const bool cross = dep && (crs[0] || crs[1] || crs[2]);
             float x2[3] = {xe[0], xe[1], xe[2]};
-            if (cross) split_point(i1, i2, xs, xe, x2);
+            if (cross) split_point(crs, xs, xe, x2);
             if (fast) {
-                float v[12];
-                pqr_mixed(i1, xs, x2, wx, wy, wz, v);
+                int w[12];
+                pqr_quant(cc, xs, x2, wx, wy, wz, inv_qs, w);
                 // Jx (0,0,0) (0,0,1) (0,1,0) (0,1,1); Jy (0,0,0) (0,0,1) (1,0,0) (1,0,1);
                 // Jz (0,0,0) (0,1,0) (1,0,0) (1,1,0) from the base node iv = i1
                 int *J = myJ + lc + ox + oy + oz;
                 const int off[12] = {0, 1, SZ, SZ + 1, nn, nn + 1, nn + SYZ, nn + SYZ + 1,
                                      2 * nn, 2 * nn + SZ, 2 * nn + SYZ, 2 * nn + SYZ + SZ};
 #pragma unroll
-                for (int q = 0; q < 12; q++) {
-                    const int w = __float_as_int(fmaf(v[q], inv_qs, 12582912.0f)) - 0x4B400000;  // round(v/q_s)
-                    if (w) atomicAdd(J + off[q], w);
-                }
+                for (int q = 0; q < 12; q++) atomicAdd(J + off[q], w[q]);
             }
             // queue the other segments (warp-aggregated positions)
             {
@@ -532,7 +588,7 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
                         pos += t2;
                     }
                     if (t2) {
-                        queue[pos][0] = make_float4(n0f, __int_as_float((i2[0] - 2) | ((i2[1] - 2) << 1) | ((i2[2] - 2) << 2)),
+                        queue[pos][0] = make_float4(n0f, __int_as_float((int)ge[0] | ((int)ge[1] << 1) | ((int)ge[2] << 2)),
                                                     x2[0], x2[1]);
                         queue[pos][1] = make_float4(x2[2], xe[0], xe[1], xe[2]);
                     }
@@ -545,26 +601,22 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
                 }
             }
 
-            // ---- new cell (Reflect cell.h:1427-1478 and migration, in cell units)
-            int ci[3] = {i, l, k};
-            const int nc[3] = {g.nx, g.ny, g.nz};
+            // ---- new cell (Reflect cell.h:1427-1478 and migration, in cell units):
+            // per axis a step of -1, 0 or +1 cell; a particle that stays in its
+            // tile cannot wrap, so its packed cell index moves by the steps
+            int dl[3];
+            float xw[3];
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-                if (xe[d] >= 1.f) {
-                    xe[d] -= 1.f;
-                    ci[d] = ci[d] + 1 == nc[d] ? 0 : ci[d] + 1;
-                } else if (xe[d] < 0.f) {
-                    xe[d] += 1.f;
-                    ci[d] = ci[d] == 0 ? nc[d] - 1 : ci[d] - 1;
-                }
-                xe[d] = fminf(fmaxf(xe[d], 0.f), kOneBelow);
+                const bool up = xe[d] >= 1.f, dn = xe[d] < 0.f;
+                dl[d] = (int)up - (int)dn;
+                xw[d] = fminf(fmaxf(xe[d] + (up ? -1.f : (dn ? 1.f : 0.f)), 0.f), kOneBelow);
             }
-            const int newcell = g.cell_of(ci[0], ci[1], ci[2]);
-            const bool stay = (unsigned)(ci[0] - i0) < (unsigned)g.tx && (unsigned)(ci[1] - l0) < (unsigned)g.ty &&
-                              (unsigned)(ci[2] - k0) < (unsigned)g.tz;
+            const bool stay = (unsigned)(i - i0 + dl[0]) < (unsigned)txe && (unsigned)(l - l0 + dl[1]) < (unsigned)tye &&
+                              (unsigned)(k - k0 + dl[2]) < (unsigned)tze;
             if (active && stay) {
-                S.cell[slot] = newcell;
-                S.ox[slot] = xe[0]; S.oy[slot] = xe[1]; S.oz[slot] = xe[2];
+                S.cell[slot] = cur.cell + dl[0] * cstr_x + dl[1] * cstr_y + dl[2];
+                S.ox[slot] = xw[0]; S.oy[slot] = xw[1]; S.oz[slot] = xw[2];
                 S.fx[slot] = pu; S.fy[slot] = pv; S.fz[slot] = pw;
             }
             // leavers: one outbox and one hole-list reservation per warp
@@ -581,11 +633,16 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
                 obase = __shfl_sync(FULL, obase, 0);
                 hbase = __shfl_sync(FULL, hbase, 0);
                 if (leave) {
+                    // the new cell, wrapped periodically
+                    int ci[3] = {i + dl[0], l + dl[1], k + dl[2]};
+                    const int nc[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+                    for (int d = 0; d < 3; d++) ci[d] = ci[d] == nc[d] ? 0 : (ci[d] < 0 ? nc[d] - 1 : ci[d]);
                     const unsigned e = obase + rank;
                     if (e < P.out_cap) {
                         OutMixed o;
-                        o.ox = xe[0]; o.oy = xe[1]; o.oz = xe[2]; o.px = pu; o.py = pv; o.pz = pw;
-                        o.cell = newcell;
+                        o.ox = xw[0]; o.oy = xw[1]; o.oz = xw[2]; o.px = pu; o.py = pv; o.pz = pw;
+                        o.cell = g.cell_of(ci[0], ci[1], ci[2]);
                         o.species = s;
                         outbox[e] = o;
                         moved++;
@@ -747,17 +804,27 @@ cudaError_t encode_field_maps(const Grid &g, float *const E[3], float *const H[3
 
 size_t push_smem_mixed(const Grid &g) { return mixed_smem(g.tx, g.ty, g.tz).total; }
 
+using PushMixedFn = void (*)(const MixedMaps, StepParams);
+// the instantiation for a grid's tile: fixed dimensions for the automatic tiles, else runtime
+static PushMixedFn push_mixed_fn(const Grid &g) {
+    if (g.tx == 4 && g.ty == 4 && g.tz == 12) return k_push_mixed<4, 4, 12>;
+    if (g.tx == 4 && g.ty == 4 && g.tz == 8) return k_push_mixed<4, 4, 8>;
+    if (g.tx == 4 && g.ty == 4 && g.tz == 4) return k_push_mixed<4, 4, 4>;
+    return k_push_mixed<0, 0, 0>;
+}
+
 size_t push_smem_total_mixed(const Grid &g) {
     cudaFuncAttributes a;
-    if (cudaFuncGetAttributes(&a, k_push_mixed) != cudaSuccess) return (size_t)-1;
+    if (cudaFuncGetAttributes(&a, push_mixed_fn(g)) != cudaSuccess) return (size_t)-1;
     return push_smem_mixed(g) + a.sharedSizeBytes;
 }
 
 cudaError_t launch_push_mixed(const StepParams &p, const MixedMaps &maps, cudaStream_t s) {
+    const PushMixedFn fn = push_mixed_fn(p.g);
     size_t smem = push_smem_mixed(p.g);
-    cudaError_t e = cudaFuncSetAttribute(k_push_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_push_mixed<<<p.g.ntiles, kMixedThreads, smem, s>>>(maps, p);
+    fn<<<p.g.ntiles, kMixedThreads, smem, s>>>(maps, p);
     return cudaGetLastError();
 }
 
