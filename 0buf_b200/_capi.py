@@ -113,6 +113,7 @@ SIGNATURES = {
     "pic_e_update": (C.c_int, [H]),
     "pic_e_ghosts": (C.c_int, [H]),
     "pic_get_cell_counts": (C.c_int, [H, I32]),
+    "pic_get_cell_particles": (C.c_int, [H, C.c_int, C.c_int, C.c_int64] + [D] * 6 + [I64, I64, I64]),
     "pic_num_particles": (C.c_int64, [H, C.c_int]),
     "pic_get_particles": (C.c_int, [H, C.c_int, C.c_int64] + [D] * 6 + [I32, I64]),
     "pic_energy": (C.c_int, [H, D]),
@@ -141,7 +142,6 @@ SIGNATURES = {
     "pic_error_string": (C.c_char_p, [C.c_int]),
     "pic_step_counters": (C.c_int, [H, I64]),
     "pic_step_timings": (C.c_int, [H, F]),
-    "pic_sort_stats": (C.c_int, [H, I64]),
     "pic_layout_info": (C.c_int, [H, I64]),
     "pic_stream": (C.c_void_p, [H]),
     "pic_forward": (C.c_int, [H, C.c_int, C.c_int]),

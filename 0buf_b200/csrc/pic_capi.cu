@@ -73,18 +73,7 @@ StepParams make_params(pic_handle *h) {
     return p;
 }
 
-void free_alt(pic_handle *h, int s) {
-    auto &S = h->sp[s];
-    dev_free(h, S.alt_cell);
-    for (float *&a : S.alt) {
-        dev_free(h, a);
-        a = nullptr;
-    }
-    S.alt_cell = nullptr;
-}
-
 void free_species(pic_handle *h, int s) {
-    free_alt(h, s);
     SpeciesView &v = h->sp[s].v;
     void *ptrs[] = {v.x, v.y, v.z, v.px, v.py, v.pz, v.ox, v.oy, v.oz, v.fx, v.fy, v.fz, v.cell, v.tile_start,
                     v.tile_count};
@@ -130,10 +119,6 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
     } else {
         float **arr[6] = {&v.ox, &v.oy, &v.oz, &v.fx, &v.fy, &v.fz};
         for (auto a : arr) CK(dev_alloc_n(h, a, n), "alloc particles");
-        // second set for the per-tile cell sort (maybe_sort), allocated with the bins
-        auto &S = h->sp[s];
-        CK(dev_alloc_n(h, &S.alt_cell, n), "alloc sort buffer");
-        for (float *&a : S.alt) CK(dev_alloc_n(h, &a, n), "alloc sort buffer");
     }
     CK(dev_alloc_n(h, &v.tile_start, (size_t)g.ntiles + 1), "alloc tile_start");
     CK(dev_alloc_n(h, &v.tile_count, (size_t)g.ntiles), "alloc tile_count");
@@ -167,20 +152,20 @@ using ScatterFn = std::function<cudaError_t(const SpeciesView &, int *)>;
 
 int build_bins_with(pic_handle *h, int s, int64_t n, int *cell, const ScatterFn &scatter, int64_t *inserted) {
     const Grid &g = h->g;
+    ScratchGuard guard(h);
     int *tc = nullptr;
-    CK(dev_alloc_n(h, &tc, (size_t)g.ntiles), "alloc tile counts");
+    CK(guard.alloc(&tc, (size_t)g.ntiles), "alloc tile counts");
     CK(cudaMemsetAsync(tc, 0, g.ntiles * sizeof(int), h->stream), "memset");
     CK(tile_histogram(g, n, cell, tc, h->stream), "tile histogram");
     std::vector<int> counts(g.ntiles);
     CK(cudaMemcpyAsync(counts.data(), tc, g.ntiles * sizeof(int), cudaMemcpyDeviceToHost, h->stream), "counts");
     CK(cudaStreamSynchronize(h->stream), "sync");
     int rc = alloc_species(h, s, counts);
-    if (rc) { dev_free(h, tc); return rc; }
+    if (rc) return rc;
     CK(cudaMemsetAsync(tc, 0, g.ntiles * sizeof(int), h->stream), "memset");
     CK(scatter(h->sp[s].v, tc), "scatter");
     CK(cudaMemcpyAsync(h->sp[s].v.tile_count, tc, g.ntiles * sizeof(int), cudaMemcpyDeviceToDevice, h->stream),
        "tile counts");
-    dev_free(h, tc);
     CK(cudaStreamSynchronize(h->stream), "sync");
     int64_t tot = 0;
     for (int c : counts) tot += c;
@@ -220,12 +205,11 @@ int tile_counts(pic_handle *h, int s, std::vector<int> &counts) {
 
 int load_device(pic_handle *h, int s, int64_t n, const double *x, const double *y, const double *z,
                 const double *px, const double *py, const double *pz, int64_t *inserted) {
+    ScratchGuard guard(h);
     int *cell = nullptr;
-    CK(dev_alloc_n(h, &cell, (size_t)(n > 0 ? n : 1)), "alloc cell");
+    CK(guard.alloc(&cell, (size_t)(n > 0 ? n : 1)), "alloc cell");
     CK(place_particles_plain(h->g, n, x, y, z, cell, h->stream), "place");
-    int rc = build_bins(h, s, n, cell, x, y, z, px, py, pz, inserted);
-    dev_free(h, cell);
-    return rc;
+    return build_bins(h, s, n, cell, x, y, z, px, py, pz, inserted);
 }
 
 // gather the live particles (+ outbox leftovers) of species s and rebuild its bins
@@ -241,14 +225,15 @@ int rebin_species(pic_handle *h, int s, unsigned n_out) {
     for (int t = 0; t < g.ntiles; t++) { dstart[t] = acc; acc += counts[t]; }
     dstart[g.ntiles] = acc;
     int64_t nmax = acc + n_out;
+    ScratchGuard guard(h);
     double *buf = nullptr;
     int *cell = nullptr;
     int64_t *ddst = nullptr;
     unsigned *ctr = nullptr;
-    CK(dev_alloc_n(h, &buf, (size_t)(nmax > 0 ? nmax : 1) * 6), "rebin buffer");
-    CK(dev_alloc_n(h, &cell, (size_t)(nmax > 0 ? nmax : 1)), "rebin cells");
-    CK(dev_alloc_n(h, &ddst, (size_t)g.ntiles + 1), "rebin starts");
-    CK(dev_alloc_n(h, &ctr, 1), "rebin counter");
+    CK(guard.alloc(&buf, (size_t)(nmax > 0 ? nmax : 1) * 6), "rebin buffer");
+    CK(guard.alloc(&cell, (size_t)(nmax > 0 ? nmax : 1)), "rebin cells");
+    CK(guard.alloc(&ddst, (size_t)g.ntiles + 1), "rebin starts");
+    CK(guard.alloc(&ctr, 1), "rebin counter");
     CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned), h->stream), "memset");
     CK(cudaMemcpyAsync(ddst, dstart.data(), (g.ntiles + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream),
        "starts");
@@ -260,12 +245,7 @@ int rebin_species(pic_handle *h, int s, unsigned n_out) {
     unsigned extra = 0;
     CK(cudaMemcpyAsync(&extra, ctr, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream), "counter");
     CK(cudaStreamSynchronize(h->stream), "sync");
-    int rc = build_bins(h, s, acc + extra, cell, x, y, z, px, py, pz, nullptr);
-    dev_free(h, buf);
-    dev_free(h, cell);
-    dev_free(h, ddst);
-    dev_free(h, ctr);
-    return rc;
+    return build_bins(h, s, acc + extra, cell, x, y, z, px, py, pz, nullptr);
 }
 
 int check_status(pic_handle *h) {
@@ -311,31 +291,6 @@ int check_status(pic_handle *h) {
         }
         CK(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), h->stream), "reset status");
         h->kin_valid = 0;
-    }
-    return PIC_OK;
-}
-
-// FP32 form: sort a species' tile bins by cell (into the alternate arrays,
-// then swap) when the last push found more than 2% of its particle slots
-// outside the first few distinct cells of their warp -- the deposit sums a
-// warp's lanes per cell, which pays off when the bins are in cell order
-int maybe_sort(pic_handle *h) {
-    h->sorts = 0;
-    if (!h->mixed) return PIC_OK;
-    for (int s = 0; s < h->cfg.nspecies; s++) {
-        auto &S = h->sp[s];
-        if (!S.loaded || S.cap_total == 0 || !S.alt_cell) continue;
-        if ((double)h->st_host->unsorted[s] <= 0.02 * (double)S.cap_total) continue;
-        SpeciesView D = S.v;
-        D.cell = S.alt_cell;
-        float **dp[6] = {&D.ox, &D.oy, &D.oz, &D.fx, &D.fy, &D.fz};
-        for (int a = 0; a < 6; a++) *dp[a] = S.alt[a];
-        CK(sort_bins_f(h->g, S.v, D, h->stream), "sort bins");
-        std::swap(S.v.cell, S.alt_cell);
-        float **vp[6] = {&S.v.ox, &S.v.oy, &S.v.oz, &S.v.fx, &S.v.fy, &S.v.fz};
-        for (int a = 0; a < 6; a++) std::swap(*vp[a], S.alt[a]);
-        h->launches += 1;
-        h->sorts += 1;
     }
     return PIC_OK;
 }
@@ -596,14 +551,13 @@ int pic_load_particles(pic_handle *h, int species, int64_t n, const double *x, c
     int rc = set_device(h);
     if (rc) return rc;
     size_t N = (size_t)(n > 0 ? n : 1);
+    ScratchGuard guard(h);
     double *buf = nullptr;
-    CK(dev_alloc_n(h, &buf, N * 6), "alloc load buffer");
+    CK(guard.alloc(&buf, N * 6), "alloc load buffer");
     const double *src[6] = {x, y, z, px, py, pz};
     for (int a = 0; a < 6; a++)
         if (n > 0) CK(cudaMemcpyAsync(buf + a * N, src[a], (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream), "H2D particles");
-    rc = load_device(h, species, n, buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N, inserted);
-    dev_free(h, buf);
-    return rc;
+    return load_device(h, species, n, buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N, inserted);
 }
 
 int pic_load_particles_device(pic_handle *h, int species, int64_t n, const double *x, const double *y,
@@ -737,12 +691,13 @@ int pic_get_particles_cells(pic_handle *h, int species, int64_t cap, int32_t *ce
     if (acc > cap) return set_err(h, PIC_ERR_ARG, "capacity too small");
     if (acc == 0) return PIC_OK;
     size_t N = (size_t)acc;
+    ScratchGuard guard(h);
     float *buf = nullptr;
     int *dcell = nullptr;
     int64_t *dd = nullptr;
-    CK(cudaMalloc(&buf, N * 6 * sizeof(float)), "alloc");
-    CK(cudaMalloc(&dcell, N * sizeof(int)), "alloc");
-    CK(cudaMalloc(&dd, (g.ntiles + 1) * sizeof(int64_t)), "alloc");
+    CK(guard.alloc(&buf, N * 6), "alloc");
+    CK(guard.alloc(&dcell, N), "alloc");
+    CK(guard.alloc(&dd, (size_t)g.ntiles + 1), "alloc");
     CK(cudaMemcpyAsync(dd, dstart.data(), (g.ntiles + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream), "H2D");
     CK(gather_from_bins_f(g, h->mixed, v, dd, dcell, buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N,
                           h->stream), "gather");
@@ -751,9 +706,6 @@ int pic_get_particles_cells(pic_handle *h, int species, int64_t cap, int32_t *ce
         if (dst[a]) CK(cudaMemcpyAsync(dst[a], buf + a * N, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "D2H");
     if (cell) CK(cudaMemcpyAsync(cell, dcell, N * sizeof(int), cudaMemcpyDeviceToHost, h->stream), "D2H");
     CK(cudaStreamSynchronize(h->stream), "sync");
-    cudaFree(buf);
-    cudaFree(dcell);
-    cudaFree(dd);
     return PIC_OK;
 }
 
@@ -949,7 +901,6 @@ int pic_step(pic_handle *h, int nt) {
     if ((rc = do_e_ghosts(h))) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     rc = check_status(h);
-    if (!rc) rc = maybe_sort(h);
     h->counters[3] = h->launches;
     if (!rc) {
         cudaEventElapsedTime(&h->timings[0], h->ev[0], h->ev[1]);
@@ -992,6 +943,60 @@ int pic_get_cell_counts(pic_handle *h, int *counts) {
     for (int i = 0; i < g.nx; i++)
         for (int l = 0; l < g.ny; l++)
             for (int k = 0; k < g.nz; k++) counts[((size_t)i * g.NY + l) * g.NZ + k] = c[g.dense_of(i, l, k)];
+    return PIC_OK;
+}
+
+int pic_get_cell_particles(pic_handle *h, int species, int cell, int64_t cap, double *x, double *y, double *z,
+                           double *px, double *py, double *pz, int64_t *slot, int64_t *n, int64_t *bin_offset) {
+    if (!h || species < 0 || species >= h->cfg.nspecies || cap < 0) return set_err(h, PIC_ERR_ARG, "bad argument");
+    const Grid &g = h->g;
+    // reference cell number ((i*(Ny+2) + l)*(Nz+2) + k) of an interior cell
+    const int k = cell % g.NZ, l = (cell / g.NZ) % g.NY, i = cell / (g.NZ * g.NY);
+    if (cell < 0 || i >= g.nx || l >= g.ny || k >= g.nz) return set_err(h, PIC_ERR_ARG, "not an interior cell");
+    int rc = set_device(h);
+    if (rc) return rc;
+    if (n) *n = 0;
+    if (bin_offset) *bin_offset = 0;
+    if (!h->sp[species].loaded) return PIC_OK;
+    const SpeciesView &v = h->sp[species].v;
+    const int t = g.tile_of_cell(i, l, k);
+    int count = 0;
+    CK(cudaMemcpyAsync(&count, v.tile_count + t, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "tile count");
+    CK(cudaStreamSynchronize(h->stream), "sync");
+    if (bin_offset) *bin_offset = h->sp[species].h_start[t];
+    const size_t N = (size_t)(count > 0 ? count : 1);
+    ScratchGuard guard(h);
+    double *buf = nullptr;
+    int64_t *dslot = nullptr;
+    unsigned *dcnt = nullptr;
+    CK(guard.alloc(&buf, 6 * N), "alloc");
+    CK(guard.alloc(&dslot, N), "alloc");
+    CK(guard.alloc(&dcnt, 1), "alloc");
+    CK(cudaMemsetAsync(dcnt, 0, sizeof(unsigned), h->stream), "memset");
+    CK(cell_particles(g, h->mixed, v, t, g.cell_of(i, l, k), (int64_t)N, buf, buf + N, buf + 2 * N, buf + 3 * N,
+                      buf + 4 * N, buf + 5 * N, dslot, dcnt, h->stream), "cell particles");
+    unsigned m = 0;
+    CK(cudaMemcpyAsync(&m, dcnt, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream), "D2H");
+    CK(cudaStreamSynchronize(h->stream), "sync");
+    std::vector<double> hb(6 * (size_t)m);
+    std::vector<int64_t> hs(m);
+    for (int a = 0; a < 6; a++)
+        if (m) CK(cudaMemcpyAsync(hb.data() + a * (size_t)m, buf + a * N, m * sizeof(double), cudaMemcpyDeviceToHost,
+                                  h->stream), "D2H");
+    if (m) CK(cudaMemcpyAsync(hs.data(), dslot, m * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream), "D2H");
+    CK(cudaStreamSynchronize(h->stream), "sync");
+    if (n) *n = m;
+    if ((int64_t)m > cap) return set_err(h, PIC_ERR_ARG, "capacity too small");
+    // slot order
+    std::vector<unsigned> ord(m);
+    for (unsigned e = 0; e < m; e++) ord[e] = e;
+    std::sort(ord.begin(), ord.end(), [&](unsigned a, unsigned b) { return hs[a] < hs[b]; });
+    double *dst[6] = {x, y, z, px, py, pz};
+    for (unsigned e = 0; e < m; e++) {
+        for (int a = 0; a < 6; a++)
+            if (dst[a]) dst[a][e] = hb[a * (size_t)m + ord[e]];
+        if (slot) slot[e] = hs[ord[e]];
+    }
     return PIC_OK;
 }
 
@@ -1130,15 +1135,6 @@ const char *pic_error_string(int status) {
 int pic_step_counters(pic_handle *h, int64_t *out4) {
     if (!h || !out4) return PIC_ERR_ARG;
     for (int i = 0; i < 4; i++) out4[i] = h->counters[i];
-    return PIC_OK;
-}
-
-int pic_sort_stats(pic_handle *h, int64_t *out2) {
-    if (!h || !out2) return PIC_ERR_ARG;
-    out2[0] = 0;
-    if (h->mixed && h->st_host)
-        for (int s = 0; s < h->cfg.nspecies; s++) out2[0] += (int64_t)h->st_host->unsorted[s];
-    out2[1] = h->sorts;
     return PIC_OK;
 }
 

@@ -130,111 +130,6 @@ __global__ void k_scatter_f(Grid g, int mixed, int64_t n, const int *__restrict_
     }
 }
 
-// Counting sort of one tile's bin by cell (cells of the tile in z-fastest
-// order), FP32 form, from the arrays of S into those of D (same tile layout).
-// The mixed push sums the deposit of lanes that share a cell per warp; cell
-// changes inside a tile rewrite a particle's cell in place, arrivals are
-// appended and departures' slots refilled from the end, which leaves the bin
-// out of cell order -- this restores it.  Lanes of a warp that share a cell
-// take one shared-memory atomic per cell (match.any), so runs of one cell
-// cost no conflicts, and the writes of a run are contiguous.  Entries whose
-// cell is not in the tile (never expected) go after the sorted ones.
-__global__ void __launch_bounds__(512, 2) k_sort_tile_f(Grid g, SpeciesView S, SpeciesView D) {
-    extern __shared__ int s_off[];  // tile cells + 1
-    __shared__ int s_wsum[32];
-    __shared__ int s_carry;
-    const int t = blockIdx.x;
-    const int tk = t % g.ntz, tl = (t / g.ntz) % g.nty, ti = t / (g.ntz * g.nty);
-    const int i0 = ti * g.tx, l0 = tl * g.ty, k0 = tk * g.tz;
-    const int nc = g.tx * g.ty * g.tz;
-    const int start = S.tile_start[t], count = S.tile_count[t];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const unsigned FULL = 0xffffffffu, lt = (1u << lane) - 1;
-    for (int c = threadIdx.x; c <= nc; c += blockDim.x) s_off[c] = 0;
-    if (threadIdx.x == 0) s_carry = 0;
-    __syncthreads();
-    auto local = [&](int cell) -> int {
-        if (cell < 0) return nc;
-        int i, l, k;
-        g.cell_ijk(cell, i, l, k);
-        int a = i - i0, b = l - l0, c = k - k0;
-        if (a < 0 || a >= g.tx || b < 0 || b >= g.ty || c < 0 || c >= g.tz) return nc;
-        return (a * g.ty + b) * g.tz + c;
-    };
-    // histogram, one atomic per distinct cell per warp (the loop is warp-uniform)
-    for (int j0 = 0; j0 < count; j0 += blockDim.x) {
-        const int j = j0 + threadIdx.x;
-        const int c = j < count ? local(S.cell[start + j]) : -1;
-        const unsigned m = __match_any_sync(FULL, c);
-        if (c >= 0 && (m & lt) == 0) atomicAdd(&s_off[c], __popc(m));
-    }
-    __syncthreads();
-    // exclusive scan of the nc + 1 counts, one block-wide pass per blockDim.x entries
-    for (int c0 = 0; c0 <= nc; c0 += blockDim.x) {
-        const int c = c0 + threadIdx.x;
-        const int v = c <= nc ? s_off[c] : 0;
-        int x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(FULL, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) s_wsum[wid] = x;
-        __syncthreads();
-        if (wid == 0) {
-            int ws = lane < nw ? s_wsum[lane] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(FULL, ws, o);
-                if (lane >= o) ws += y;
-            }
-            if (lane < nw) s_wsum[lane] = ws;  // inclusive over warps
-        }
-        __syncthreads();
-        const int carry = s_carry;
-        const int excl = carry + (wid > 0 ? s_wsum[wid - 1] : 0) + x - v;
-        if (c <= nc) s_off[c] = excl;
-        __syncthreads();
-        if (threadIdx.x == 0) s_carry = carry + s_wsum[nw - 1];
-        __syncthreads();
-    }
-    // scatter: the first lane of each run of one cell reserves the run's slots;
-    // two entries per thread per pass, all loads issued before the writes
-    struct Ent {
-        int cell;
-        float v[6];
-    };
-    auto load_ent = [&](int j, int &c, Ent &e) {
-        c = j < count ? local(S.cell[start + j]) : -1;
-        if (c >= 0) {
-            const int src = start + j;
-            e.cell = S.cell[src];
-            e.v[0] = S.ox[src]; e.v[1] = S.oy[src]; e.v[2] = S.oz[src];
-            e.v[3] = S.fx[src]; e.v[4] = S.fy[src]; e.v[5] = S.fz[src];
-        }
-    };
-    auto place = [&](int c, const Ent &e) {
-        const unsigned m = __match_any_sync(FULL, c);
-        const int first = __ffs(m) - 1;
-        int base = 0;
-        if (c >= 0 && lane == first) base = atomicAdd(&s_off[c], __popc(m));
-        base = __shfl_sync(FULL, base, first);
-        if (c >= 0) {
-            const int dst = start + base + __popc(m & lt);
-            D.cell[dst] = e.cell;
-            D.ox[dst] = e.v[0]; D.oy[dst] = e.v[1]; D.oz[dst] = e.v[2];
-            D.fx[dst] = e.v[3]; D.fy[dst] = e.v[4]; D.fz[dst] = e.v[5];
-        }
-    };
-    for (int j0 = 0; j0 < count; j0 += 2 * blockDim.x) {
-        int c0, c1;
-        Ent e0, e1;
-        load_ent(j0 + threadIdx.x, c0, e0);
-        load_ent(j0 + blockDim.x + threadIdx.x, c1, e1);
-        place(c0, e0);
-        place(c1, e1);
-    }
-    // free slots of the tile stay marked empty in the new arrays
-    for (int j = start + count + threadIdx.x; j < S.tile_start[t + 1]; j += blockDim.x) D.cell[j] = -1;
-}
 
 __global__ void k_gather_f(Grid g, int mixed, SpeciesView S, const int64_t *__restrict__ dense_start, int *cell,
                            float *ox, float *oy, float *oz, float *px, float *py, float *pz) {
@@ -319,6 +214,31 @@ __global__ void k_cell_hist(StepParams P, int *counts) {
         int i, l, k;
         cell_ijk(P.g, c, i, l, k);
         if (i < P.g.nx && l < P.g.ny && k < P.g.nz) atomicAdd(&counts[P.g.dense_of(i, l, k)], 1);
+    }
+}
+
+// the particles of one packed cell in one tile's bin, in no particular order
+// (the host sorts them by slot): FP64 global positions and momenta and the slot
+__global__ void k_cell_particles(Grid g, int mixed, SpeciesView S, int t, int cell, int64_t cap, double *x, double *y,
+                                 double *z, double *px, double *py, double *pz, int64_t *slot, unsigned *count) {
+    const int start = S.tile_start[t], n = S.tile_count[t];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int q = start + j;
+        if (S.cell[q] != cell) continue;
+        const unsigned e = atomicAdd(count, 1u);
+        if (e >= cap) continue;
+        slot[e] = q;
+        if (!mixed) {
+            x[e] = S.x[q]; y[e] = S.y[q]; z[e] = S.z[q];
+            px[e] = S.px[q]; py[e] = S.py[q]; pz[e] = S.pz[q];
+        } else {
+            int i, l, k;
+            cell_ijk(g, cell, i, l, k);
+            x[e] = ((double)i + (double)S.ox[q]) * g.hx;
+            y[e] = ((double)l + (double)S.oy[q]) * g.hy;
+            z[e] = ((double)k + (double)S.oz[q]) * g.hz;
+            px[e] = S.fx[q]; py[e] = S.fy[q]; pz[e] = S.fz[q];
+        }
     }
 }
 
@@ -557,15 +477,6 @@ cudaError_t scatter_to_bins_f(const Grid &g, int mixed, int64_t n, const int *ce
     return cudaGetLastError();
 }
 
-cudaError_t sort_bins_f(const Grid &g, const SpeciesView &src, const SpeciesView &dst, cudaStream_t s) {
-    size_t smem = ((size_t)g.tx * g.ty * g.tz + 1) * sizeof(int);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_sort_tile_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    k_sort_tile_f<<<g.ntiles, 512, smem, s>>>(g, src, dst);
-    return cudaGetLastError();
-}
 
 cudaError_t gather_from_bins_f(const Grid &g, int mixed, SpeciesView sv, const int64_t *dense_start, int *cell,
                                float *ox, float *oy, float *oz, float *px, float *py, float *pz, cudaStream_t s) {
@@ -590,6 +501,13 @@ cudaError_t cell_histogram(const StepParams &p, int *counts, cudaStream_t s) {
 cudaError_t gather_from_bins(const Grid &g, int mixed, SpeciesView sv, const int64_t *dense_start, double *x,
                              double *y, double *z, double *px, double *py, double *pz, int *cell, cudaStream_t s) {
     k_gather<<<g.ntiles, 256, 0, s>>>(g, mixed, sv, dense_start, x, y, z, px, py, pz, cell);
+    return cudaGetLastError();
+}
+
+cudaError_t cell_particles(const Grid &g, int mixed, const SpeciesView &sv, int tile, int cell, int64_t cap, double *x,
+                           double *y, double *z, double *px, double *py, double *pz, int64_t *slot, unsigned *count,
+                           cudaStream_t s) {
+    k_cell_particles<<<64, 256, 0, s>>>(g, mixed, sv, tile, cell, cap, x, y, z, px, py, pz, slot, count);
     return cudaGetLastError();
 }
 

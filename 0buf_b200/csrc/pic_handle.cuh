@@ -26,15 +26,10 @@ struct pic_handle {
         int64_t cap_total;
         int loaded;
         std::vector<int> h_start;
-        // FP32 form: second set of particle arrays (same capacity) that the
-        // per-tile cell sort writes into before the two sets swap
-        int *alt_cell;
-        float *alt[6];
         // FP32 form: the bound of its contributions is known from a push
         // (cleared whenever the bins are rebuilt)
         int lb_known;
     } sp[pic::kMaxSpecies];
-    int64_t sorts;  // tile sorts run by the last step
     void *outbox;
     unsigned out_cap;
     int outbox_pinned;  // set while a multi-species rebin still reads leftovers from the outbox
@@ -86,6 +81,22 @@ template <class T>
 cudaError_t dev_alloc_n(pic_handle *h, T **p, size_t n) {
     return dev_alloc(h, (void **)p, n * sizeof(T));
 }
+// device buffers freed when the guard leaves scope, so that an error return
+// (CK) between allocation and release leaks nothing
+struct ScratchGuard {
+    pic_handle *h;
+    std::vector<void *> bufs;
+    explicit ScratchGuard(pic_handle *hh) : h(hh) {}
+    template <class T>
+    cudaError_t alloc(T **p, size_t n) {
+        cudaError_t e = dev_alloc(h, (void **)p, n * sizeof(T));
+        if (e == cudaSuccess) bufs.push_back((void *)*p);
+        return e;
+    }
+    ~ScratchGuard() {
+        for (void *p : bufs) dev_free(h, p);
+    }
+};
 // kernel parameters of the current state (species views, fields, outbox, status)
 pic::StepParams make_params(pic_handle *h);
 // flat device list of one species (packed cell, FP64 global positions and

@@ -48,9 +48,6 @@ struct DevStatus {
     unsigned long long duplicated;
     double kinetic;            // sum (m/q_m)(gamma-1) accumulated by the push
     double pad1[3];
-    // mixed push, per species: depositing particles beyond the first kGroups
-    // distinct cells of their warp (bins out of cell order)
-    unsigned long long unsorted[kMaxSpecies];
 };
 
 struct Grid {

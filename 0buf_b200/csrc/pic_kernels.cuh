@@ -41,8 +41,6 @@ cudaError_t scatter_to_bins_f(const Grid &g, int mixed, int64_t n, const int *ce
                               int *fill, cudaStream_t s);
 cudaError_t gather_from_bins_f(const Grid &g, int mixed, SpeciesView sv, const int64_t *dense_start, int *cell,
                                float *ox, float *oy, float *oz, float *px, float *py, float *pz, cudaStream_t s);
-// FP32 form: sort each tile's bin by cell from src's arrays into dst's (same tile layout)
-cudaError_t sort_bins_f(const Grid &g, const SpeciesView &src, const SpeciesView &dst, cudaStream_t s);
 // flat device list -> per-tile counts of valid particles (cell >= 0)
 cudaError_t tile_histogram(const Grid &g, int64_t n, const int *cell, int *tile_counts, cudaStream_t s);
 // flat FP64 list -> bins of one species (plain or mixed), fill[] = running counts
@@ -52,6 +50,10 @@ cudaError_t scatter_to_bins(const Grid &g, int mixed, int64_t n, const int *cell
 // bins of one species -> flat list in slot order (global FP64 positions)
 cudaError_t gather_from_bins(const Grid &g, int mixed, SpeciesView sv, const int64_t *dense_start, double *x,
                              double *y, double *z, double *px, double *py, double *pz, int *cell, cudaStream_t s);
+// the particles of one packed cell of tile `tile` (at most cap), count in *count
+cudaError_t cell_particles(const Grid &g, int mixed, const SpeciesView &sv, int tile, int cell, int64_t cap, double *x,
+                           double *y, double *z, double *px, double *py, double *pz, int64_t *slot, unsigned *count,
+                           cudaStream_t s);
 // outbox leftovers of one species (after a failed insert) -> flat list appended at offset
 cudaError_t gather_outbox(const StepParams &p, int species, unsigned n_out, unsigned *counter, int64_t offset,
                           double *x, double *y, double *z, double *px, double *py, double *pz, int *cell,

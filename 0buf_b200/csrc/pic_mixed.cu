@@ -268,8 +268,6 @@ constexpr int kJCopies = kMixedWarps / 2;         // int32 tile currents per CTA
 constexpr int kQueue = PIC_MIXED_QUEUE;           // queued segments per warp
 static_assert(kMixedThreads % 32 == 0, "whole warps");
 static_assert(kQueue >= 64, "one iteration can queue two segments per lane");
-static_assert(kHoleMax * sizeof(int) <= kMixedWarps * kQueue * 2 * sizeof(float4),
-              "the compaction's front-hole list lives in the queues' memory");
 
 // w (in units of 2^e_w) -> units of 2^e_tile, sh = e_w - e_tile, round half up
 __device__ __forceinline__ long long rescale(long long w, int sh) {
@@ -295,7 +293,7 @@ __host__ __device__ inline MixedSmem mixed_smem(int tx, int ty, int tz) {
     m.quads = round_up_sz(raw_bytes > jw_bytes ? raw_bytes : jw_bytes, 128);
     m.tilej = m.quads + 6 * nn * sizeof(float4);
     m.holes = m.tilej + 3 * nn * sizeof(unsigned long long);
-    m.total = m.holes + kHoleMax * sizeof(int);
+    m.total = m.holes + 2 * kHoleMax * sizeof(int);  // holes, then the front holes
     return m;
 }
 
@@ -306,9 +304,13 @@ template <int TX, int TY, int TZ>
 __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps maps, StepParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long sBar;
-    __shared__ int sNHoles, sNFront, sNMove;
+    // hole-list counters in three sets by species (s mod 3), so that a species
+    // needs no barrier before its loop: thread 0 clears the set of species s+1
+    // before the end barrier of species s, after the last use of that set
+    // (species s-2's compaction, before the end barrier of species s-1)
+    __shared__ int sNHoles[3], sNFront[3], sNMove[3];
     __shared__ double sRed[kMixedWarps];
-    __shared__ unsigned sLbMax;
+    __shared__ unsigned sLbMax[kMaxSpecies];
     __shared__ double sQ;
     __shared__ int sTileE;
     __shared__ float sInvQ;
@@ -331,8 +333,7 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     unsigned long long *sJ = (unsigned long long *)(smem_raw + L.tilej);
     int *sJw = (int *)(smem_raw + L.jw);
     int *sHoles = (int *)(smem_raw + L.holes);
-    // the front-hole list of the compaction reuses the (then drained) queues
-    int *sFront = (int *)&sQueue[0][0][0];
+    int *sFront = sHoles + kHoleMax;  // the compaction's holes in front of the new count
     int *myJ = sJw + (warp % kJCopies) * 3 * nn;
 
     // a TMA destination starts on a 128-byte boundary (block-uniform check)
@@ -379,7 +380,8 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < kJCopies * 3 * nn; idx += blockDim.x) sJw[idx] = 0;
-    if (threadIdx.x == 0) sLbMax = 0u;
+    if (threadIdx.x < kMaxSpecies) sLbMax[threadIdx.x] = 0u;
+    if (threadIdx.x < 3) { sNHoles[threadIdx.x] = 0; sNFront[threadIdx.x] = 0; sNMove[threadIdx.x] = 0; }
     __syncthreads();
     const float inv_q = sInvQ;
     const int tile_e = sTileE;
@@ -398,6 +400,7 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
 
     for (int s = 0; s < P.nsp; s++) {
         const SpeciesView &S = P.sp[s];
+        const int sp = s % 3;  // hole-list counters of this species
         const int start = S.tile_start[t];
         const int count = S.tile_count[t];
         const float tau1 = (float)(S.q_m * g.tau * 0.5);
@@ -409,7 +412,8 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
         const float light = 1.0834f * fmaxf(fabsf(wx) * ctx, fmaxf(fabsf(wy) * cty, fabsf(wz) * ctz));
         const float prev = P.lb_prev ? P.lb_prev[s] : 0.f;
         const float cmax = prev > 0.f ? fminf(2.f * prev, light) : light;
-        // int32 quantum 2^e_s >= 2^-22 cmax
+        // int32 quantum 2^e_s >= 2^-22 cmax, per species: one quantum for
+        // species of very different speeds would round the slow ones coarsely
         const int e_s = max(exponent_above(cmax * 0x1p-22f), -100);
         const float inv_qs = pow2f(-e_s);
         const int sh = e_s - tile_e;  // int32 quantum / tile quantum = 2^sh
@@ -425,8 +429,6 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             }
             __syncwarp();
         };
-        if (threadIdx.x == 0) { sNHoles = 0; sNFront = 0; sNMove = 0; }
-        __syncthreads();
         int qn = 0;  // segments in this warp's queue (warp-uniform)
         float lbmax = 0.f;
         // deposit the queued segments [from, from + n), one per lane, into the tile J
@@ -493,24 +495,25 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             float fHy = interp_quad2(sF + 4 * nn + lc + oy, SYZ, nx, ky, nz);
             float fHz = interp_quad2(sF + 5 * nn + lc + oz, SYZ, nx, ny, kz);
 
-            // ---- Particle::Move (particle.h:65-202), FP32
+            // ---- Particle::Move (particle.h:65-202), FP32: the half electric
+            // kick, the magnetic rotation, the second half kick.  The reference
+            // writes the rotation as the matrix (I + b b^T + [b]x) / (1 + b^2)
+            // applied to p + p x b; here it is the algebraically identical
+            // two-cross-product form p+ = p + (p + p x b) x (2 b / (1 + b^2)),
+            // with fewer operations
             pu += tau1 * fEx;
             pv += tau1 * fEy;
             pw += tau1 * fEz;
             float ps = tau1 * rsqrtf(pu * pu + pv * pv + pw * pw + 1.f);
             {
-                float bx = ps * fHx, by = ps * fHy, bz = ps * fHz;
-                float su = pu + pv * bz - pw * by;
-                float sv = pv + pw * bx - pu * bz;
-                float sw = pw + pu * by - pv * bx;
-                float q1 = bx * bx, q2 = by * by, q3 = bz * bz, q4 = bx * by, q5 = by * bz, q6 = bz * bx;
-                float rs = __fdividef(1.f, q1 + 1.f + q2 + q3);
-                float pu1 = ((q1 + 1.f) * su + (q4 + bz) * sv + (q6 - by) * sw) * rs;
-                float pv1 = ((q4 - bz) * su + (q2 + 1.f) * sv + (q5 + bx) * sw) * rs;
-                float pw1 = ((q6 + by) * su + (q5 - bx) * sv + (q3 + 1.f) * sw) * rs;
-                pu = pu1 + fEx * tau1;
-                pv = pv1 + fEy * tau1;
-                pw = pw1 + fEz * tau1;
+                const float bx = ps * fHx, by = ps * fHy, bz = ps * fHz;
+                const float f = __fdividef(2.f, 1.f + bx * bx + by * by + bz * bz);
+                const float su = pu + (pv * bz - pw * by);
+                const float sv = pv + (pw * bx - pu * bz);
+                const float sw = pw + (pu * by - pv * bx);
+                pu += f * (sv * bz - sw * by) + fEx * tau1;
+                pv += f * (sw * bx - su * bz) + fEy * tau1;
+                pw += f * (su * by - sv * bx) + fEz * tau1;
             }
             float p2 = pu * pu + pv * pv + pw * pw;
             float ig = rsqrtf(p2 + 1.f);
@@ -628,7 +631,7 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
                 int hbase = 0;
                 if (lane == 0) {
                     obase = atomicAdd(&P.st->out_count, (unsigned)nl);
-                    hbase = atomicAdd(&sNHoles, nl);
+                    hbase = atomicAdd(&sNHoles[sp], nl);
                 }
                 obase = __shfl_sync(FULL, obase, 0);
                 hbase = __shfl_sync(FULL, hbase, 0);
@@ -660,12 +663,12 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
         drain_range(0, qn);
         // the species' largest contribution bound, for the next push's quantum
         lbmax = __uint_as_float(__reduce_max_sync(FULL, __float_as_uint(lbmax)));
-        if (lane == 0 && lbmax > 0.f) atomicMax(&sLbMax, __float_as_uint(lbmax));
-        __syncthreads();
-        if (threadIdx.x == 0 && P.lb_cur && sLbMax) {
-            atomicMax(&P.lb_cur[s], sLbMax);
-            sLbMax = 0u;
+        if (lane == 0 && lbmax > 0.f) atomicMax(&sLbMax[s], __float_as_uint(lbmax));
+        if (threadIdx.x == 0) {
+            const int nx3 = (s + 1) % 3;
+            sNHoles[nx3] = 0; sNFront[nx3] = 0; sNMove[nx3] = 0;
         }
+        __syncthreads();
         // int32 currents of the species -> exact 64-bit tile J; clear them
         for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
             long long sum = 0;
@@ -676,19 +679,21 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             }
             if (sum) sJ[idx] += (unsigned long long)rescale(sum, sh);
         }
-        const int nh = sNHoles;
+        // compaction: the last live particles of the bin move into the holes in
+        // front of the new count
+        const int nh = sNHoles[sp];
         if (nh > 0 && nh <= kHoleMax) {
             const int newcount = count - nh;
             for (int r = threadIdx.x; r < nh; r += blockDim.x) {
                 int h = sHoles[r];
-                if (h < newcount) sFront[atomicAdd(&sNFront, 1)] = h;
+                if (h < newcount) sFront[atomicAdd(&sNFront[sp], 1)] = h;
             }
             __syncthreads();
             for (int r = threadIdx.x; r < nh; r += blockDim.x) {
                 int src = start + newcount + r;
                 if (S.cell[src] >= 0) {
-                    int mv = atomicAdd(&sNMove, 1);
-                    if (mv >= sNFront) { bad |= ST_BADCELL; continue; }
+                    int mv = atomicAdd(&sNMove[sp], 1);
+                    if (mv >= sNFront[sp]) { bad |= ST_BADCELL; continue; }
                     int dst = start + sFront[mv];
                     S.cell[dst] = S.cell[src];
                     S.ox[dst] = S.ox[src]; S.oy[dst] = S.oy[src]; S.oz[dst] = S.oz[src];
@@ -697,8 +702,11 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             }
             if (threadIdx.x == 0) S.tile_count[t] = newcount;
         }
+        // the next species adds into the cleared int32 currents
         __syncthreads();
     }
+    if (threadIdx.x < P.nsp && P.lb_cur && sLbMax[threadIdx.x]) atomicMax(&P.lb_cur[threadIdx.x], sLbMax[threadIdx.x]);
+    __syncthreads();
 
     for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
         long long iv = (long long)sJ[idx];

@@ -81,7 +81,9 @@ extern "C" int pic_field_energy_noalloc(int nx, int ny, int nz, const double *Ex
                                         const double *Hx, const double *Hy, const double *Hz, double *out3,
                                         void *stream) {
     if (nx < 1 || ny < 1 || nz < 1 || !Ex || !Ey || !Ez || !Hx || !Hy || !Hz || !out3) return PIC_ERR_ARG;
-    const long long nodes = (long long)(nx + 2) * (ny + 2) * (nz + 2);
+    // each extent alone must fit the scratch before any product is formed
+    if (nx > PIC_NOALLOC_MAX_NODES || ny > PIC_NOALLOC_MAX_NODES || nz > PIC_NOALLOC_MAX_NODES) return PIC_ERR_ARG;
+    const long long nodes = ((long long)nx + 2) * ((long long)ny + 2) * ((long long)nz + 2);
     const long long nblocks = (nodes + kThreads - 1) / kThreads;
     if (nblocks > PIC_NOALLOC_MAX_BLOCKS) return PIC_ERR_ARG;  // more than PIC_NOALLOC_MAX_NODES nodes
     int dev = 0;
@@ -101,8 +103,13 @@ extern "C" int pic_field_energy_noalloc(int nx, int ny, int nz, const double *Ex
         }
         partials = g_addr[dev];
     }
+    // an error left by the caller's own earlier work is reported as such, not
+    // as a failure of these launches (cudaPeekAtLastError does not clear it)
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return (int)e;
     cudaStream_t s = (cudaStream_t)stream;
     k_energy_partials<<<(unsigned)nblocks, kThreads, 0, s>>>(nx, ny, nz, Ex, Ey, Ez, Hx, Hy, Hz, nodes, partials);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     k_energy_finish<<<1, kThreads, 0, s>>>(partials, (int)nblocks, out3);
     return (int)cudaGetLastError();
 }

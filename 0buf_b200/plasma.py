@@ -146,6 +146,28 @@ class PicSimulation:
         self._ck(self.lib.pic_get_cell_counts(self.h, iptr(c)), "pic_get_cell_counts")
         return c
 
+    def cell_particles(self, species: int, cell: int) -> dict:
+        """One interior cell's particles of one species (pic_get_cell_particles):
+        x y z px py pz (global FP64) and slot in slot order, plus the tile bin's
+        first slot; cell is the reference cell number."""
+        n = C.c_int64(0)
+        off = C.c_int64(0)
+        # first call for the count (cap 0 returns PIC_ERR_ARG when the cell holds particles)
+        rc = self.lib.pic_get_cell_particles(self.h, species, int(cell), 0, *([None] * 6), None, C.byref(n), C.byref(off))
+        m = int(n.value)
+        if rc != 0 and m == 0:
+            self._ck(rc, "pic_get_cell_particles")
+        out = {k: np.zeros(max(m, 1)) for k in ("x", "y", "z", "px", "py", "pz")}
+        slot = np.zeros(max(m, 1), np.int64)
+        self._ck(self.lib.pic_get_cell_particles(self.h, species, int(cell), m, *[dptr(out[k]) for k in
+                                                 ("x", "y", "z", "px", "py", "pz")], slot.ctypes.data_as(
+                                                 C.POINTER(C.c_int64)), C.byref(n), C.byref(off)),
+                 "pic_get_cell_particles")
+        res = {k: v[:m] for k, v in out.items()}
+        res["slot"] = slot[:m]
+        res["bin_offset"] = int(off.value)
+        return res
+
     # -------------------------------------------------------------- fields
     def get_field(self, name: str) -> np.ndarray:
         a = np.zeros(int(np.prod(self.shape)))

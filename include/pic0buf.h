@@ -188,6 +188,17 @@ int pic_e_ghosts(pic_handle *h);
 /* Particle counts per cell over all species, reference numbering,
  * (Nx+2)(Ny+2)(Nz+2) ints (ghost cells 0). */
 int pic_get_cell_counts(pic_handle *h, int *counts);
+/* One cell's particles of one species: the counterpart of reading a GPUCell
+ * back to the host (GPUCell::copyCellFromDevice, gpucell.h:290-427).  cell is
+ * the reference cell number ((i*(Ny+2) + l)*(Nz+2) + k) of an interior cell.
+ * Particles live in tile bins, so a cell's particles are the slots of its
+ * tile's bin that carry its cell index.  Writes up to cap particles in slot
+ * order (global FP64 positions and momenta in either form; NULL arrays are
+ * skipped) and their slots (indices into the species' bin storage);
+ * *n = the cell's particle count (returned also when it exceeds cap, which is
+ * PIC_ERR_ARG), *bin_offset = the first slot of the tile's bin. */
+int pic_get_cell_particles(pic_handle *h, int species, int cell, int64_t cap, double *x, double *y, double *z,
+                           double *px, double *py, double *pz, int64_t *slot, int64_t *n, int64_t *bin_offset);
 int64_t pic_num_particles(pic_handle *h, int species); /* species < 0: all; negative on error */
 /* Exports one species to host arrays (capacity cap); positions are global
  * FP64 (the mixed form converts cell + offset).  cell gets the reference cell
@@ -314,9 +325,13 @@ int pic_adjoint_free(pic_handle *h);
  * (1.5 MB) that every GPU loading the library holds until exit; at most
  * PIC_NOALLOC_MAX_NODES nodes, larger grids return PIC_ERR_ARG.  The first
  * call on a device looks the array's device address up (cudaGetSymbolAddress),
- * so make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU (other streams, other threads) race;
- * serialise them.  The result is deterministic (fixed-order sums). */
+ * so make that first call before any stream capture.  The address is kept for
+ * the life of the process: it assumes the device's primary context lives as
+ * long, so do not call this after cudaDeviceReset on that device.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other
+ * threads) race; serialise them.  The result is deterministic (fixed-order
+ * sums).  A CUDA error pending from the caller's own earlier work is returned
+ * before anything is launched. */
 #define PIC_NOALLOC_MAX_BLOCKS 65536
 #define PIC_NOALLOC_MAX_NODES (PIC_NOALLOC_MAX_BLOCKS * 256)
 int pic_field_energy_noalloc(int nx, int ny, int nz, const double *Ex, const double *Ey, const double *Ez,
@@ -410,13 +425,6 @@ const char *pic_error_string(int status);
  * [1] particles no cell accepted (dropped), [2] particles two or more cells
  * accepted (duplicated), [3] kernel launches of the step. */
 int pic_step_counters(pic_handle *h, int64_t *out4);
-/* Bin order of the FP32 form after the last step: [0] depositing particles
- * that the push found outside the first few distinct cells of their warp
- * (they take the slower per-particle deposit), [1] per-tile cell sorts the
- * step ran (the bins are re-sorted by cell when [0] exceeds 2% of the
- * particle slots).  Both are 0 in the FP64 form.  No counterpart in the
- * reference, whose per-cell particle arrays are always grouped by cell. */
-int pic_sort_stats(pic_handle *h, int64_t *out2);
 /* Timings of the last pic_step in milliseconds (CUDA events on the handle's
  * stream): [0] B half step, [1] the push/deposit kernel alone, [2] migration
  * arrivals, [3] J fold + B completion + E update + E ghosts, [4] whole step. */

@@ -135,4 +135,5 @@ def test_long_run_conserves_particles_and_charge(pkg, precision, tol):
         sim.run(1000)
         assert [sim.num_particles(s) for s in range(3)] == n0
         g = sim.gauss_check()
+        print(f"{precision}: 1000-step Gauss drift max|G - G0| / max|rho| = {g[0] / g[1]:.3e}")
         assert g[0] < tol * g[1], g

@@ -52,6 +52,19 @@ def test_field_energy_noalloc_matches(pkg):
         assert not np.array_equal(first, second)
         _check(sim, second)
 
+        # on a caller's own stream: enqueued there, ready once that stream is synchronised
+        stream = torch.cuda.Stream()
+        dev = [torch.from_numpy(np.ascontiguousarray(sim.get_field(f))).cuda() for f in FIELDS]
+        out = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        rc = lib.pic_field_energy_noalloc(*cells, *[t.data_ptr() for t in dev], out.data_ptr(),
+                                          C.c_void_p(stream.cuda_stream))
+        assert rc == 0, lib.pic_error_string(rc)
+        stream.synchronize()
+        _check(sim, out.cpu().numpy())
+
         # a grid beyond the static scratch is refused before any device work
+        rc = lib.pic_field_energy_noalloc(2 ** 31 - 2, 4, 4, *([C.c_void_p(1)] * 7), None)
+        assert pkg._capi.PIC_ERR.get(rc) == "PIC_ERR_ARG"
         rc = lib.pic_field_energy_noalloc(4096, 4096, 4096, *([C.c_void_p(1)] * 7), None)
         assert pkg._capi.PIC_ERR.get(rc) == "PIC_ERR_ARG"
