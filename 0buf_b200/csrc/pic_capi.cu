@@ -317,7 +317,7 @@ int do_b_half(pic_handle *h) {
     return PIC_OK;
 }
 
-int do_push_deposit(pic_handle *h) {
+int do_push_deposit(pic_handle *h, int b_half_in_push = 0) {
     int rc = need_particles(h);
     if (rc) return rc;
     size_t nodes = h->g.nodes_pitched();
@@ -338,6 +338,7 @@ int do_push_deposit(pic_handle *h) {
            "reset bounds");
     }
     StepParams p = make_params(h);
+    p.b_half = b_half_in_push;
     cudaEventRecord(h->ev[2], h->stream);
     CK(h->mixed ? launch_push_mixed(p, h->maps, h->stream) : launch_push_plain(p, h->stream), "push_deposit");
     cudaEventRecord(h->ev[3], h->stream);
@@ -499,6 +500,7 @@ int pic_create(const pic_config *cfg, pic_handle **out) {
         if ((e = encode_field_maps(g, (float *const *)&h->f[PIC_EX], (float *const *)&h->f[PIC_HX], &h->maps)) !=
             cudaSuccess)
             return fail(e);
+
         if ((e = cudaMalloc(&h->lb_buf, 2 * kMaxSpecies * sizeof(float))) != cudaSuccess) return fail(e);
         if ((e = cudaMemsetAsync(h->lb_buf, 0, 2 * kMaxSpecies * sizeof(float), h->stream)) != cudaSuccess)
             return fail(e);
@@ -531,6 +533,7 @@ int pic_destroy(pic_handle *h) {
     if (h->hred) cudaFreeHost(h->hred);
     if (h->dcounts) cudaFree(h->dcounts);
     if (h->lb_buf) cudaFree(h->lb_buf);
+
     double *diag[3] = {h->rho, h->gauss, h->gauss0};
     for (double *d : diag)
         if (d) cudaFree(d);
@@ -888,15 +891,23 @@ int pic_step(pic_handle *h, int nt) {
     if (rc) return rc;
     h->launches = 0;
     cudaEventRecord(h->ev[0], h->stream);
-    if ((rc = do_b_half(h))) return rc;
+    // the FP32 form forms the B half step inside the push's staged field tile
+    if (!h->mixed && (rc = do_b_half(h))) return rc;
     cudaEventRecord(h->ev[1], h->stream);
-    if ((rc = do_push_deposit(h))) return rc;  // records ev[2], ev[3] around the kernel
+    if ((rc = do_push_deposit(h, h->mixed))) return rc;  // records ev[2], ev[3] around the kernel
     StepParams p = make_params(h);
     CK(launch_insert(p, h->stream), "insert");
     h->launches += 2;
     cudaEventRecord(h->ev[4], h->stream);
     if ((rc = do_j_fold(h))) return rc;
-    if ((rc = do_b_complete(h))) return rc;
+    if (h->mixed) {
+        // H in memory is still the full-step field: both half steps in one pass
+        yee_b_both_mixed(h->g, (float *const *)&h->f[PIC_EX], (float *const *)&h->f[PIC_HX], h->stream);
+        CK(cudaGetLastError(), "b_complete");
+        h->launches += 1;
+    } else if ((rc = do_b_complete(h))) {
+        return rc;
+    }
     if ((rc = do_e_update(h))) return rc;
     if ((rc = do_e_ghosts(h))) return rc;
     cudaEventRecord(h->ev[5], h->stream);

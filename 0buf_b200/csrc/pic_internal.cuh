@@ -158,6 +158,10 @@ struct StepParams {
     // atomicMax); sizes the int32 tile current's quantum
     const float *lb_prev;
     unsigned *lb_cur;
+    // mixed push: nonzero when H in memory is the full-step field and the
+    // push forms the B half step of its staged tile itself (pic_step); zero
+    // when the sub-step call pic_b_half has already advanced H
+    int b_half;
 };
 
 // FP32 form: TMA descriptors of the six E/H field arrays (3D {Nz+2, Ny+2,

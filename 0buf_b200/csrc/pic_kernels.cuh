@@ -20,6 +20,8 @@ cudaError_t place_particles_plain(const Grid &g, int64_t n, const double *x, con
 
 // mixed form (pic_mixed.cu, FP32 with FP64 global J)
 void yee_b_half_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s);
+// both B half steps of a step in one pass, H = (H + Q(E)) + Q(E) (pic_step: the push forms the first in shared memory)
+void yee_b_both_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s);
 void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], double *const J[3], cudaStream_t s);
 size_t push_smem_mixed(const Grid &g);
 // dynamic + static shared memory of the mixed push kernel ((size_t)-1 if it cannot be queried)

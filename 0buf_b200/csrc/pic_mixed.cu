@@ -20,20 +20,70 @@ namespace {
 constexpr float kOneBelow = 0.99999994f;  // largest float < 1
 
 // ------------------------------------------------------------------ Yee --
+// The element updates with every product and sum rounded on its own (no FMA
+// contraction), so that every kernel forming them -- the B and E kernels and
+// the push's staging of the half step -- gets the same bits.
+// emh1_Element (kernels.cu:1052-1073): Q = 1/2 (c1 (a1 - b1) - c2 (a2 - b2))
+__device__ __forceinline__ float q_half(float c1, float a1, float b1, float c2, float a2, float b2) {
+    return __fmul_rn(0.5f, __fsub_rn(__fmul_rn(c1, __fsub_rn(a1, b1)), __fmul_rn(c2, __fsub_rn(a2, b2))));
+}
+// emeElement (kernels.cu:1091-1102): E + ((c1 (a1 - b1) - c2 (a2 - b2)) - tau J), tau J formed in FP64
+__device__ __forceinline__ float e_step(float e, float c1, float a1, float b1, float c2, float a2, float b2, double tj) {
+    return __fadd_rn(e, __fsub_rn(__fsub_rn(__fmul_rn(c1, __fsub_rn(a1, b1)), __fmul_rn(c2, __fsub_rn(a2, b2))),
+                                  (float)tj));
+}
+
+// Four consecutive z nodes per thread, 128-bit loads and stores (rows start
+// on 16 bytes: the z pitch is a multiple of 4), one x plane per blockIdx.y;
+// the element arithmetic per node is unchanged.
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ void st4(float *p, const float v[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void un4(float4 a, float v[4]) { v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; }
+
 // H += Q(E) in FP32 (emh1_Element, kernels.cu:1052-1073; used for both the
-// half step and the completion, which adds the same Q again, kernels.cu:1024-1049)
+// half step and the completion, which adds the same Q again, kernels.cu:1024-1049).
+// TWICE: both in one pass, H = (H + Q) + Q -- pic_step's completion, whose
+// half step the push formed in shared memory only (the same bits as the two
+// separate passes of the sub-step calls)
+template <bool TWICE>
 __global__ void k_b_half_mixed(Grid g, const float *__restrict__ Ex, const float *__restrict__ Ey,
                                const float *__restrict__ Ez, float *Hx, float *Hy, float *Hz, float cx, float cy,
                                float cz) {
-    // one thread per node of an x plane (l, k flattened: no idle z tail)
+    const int nq = g.pz / 4;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= g.NY * g.NZ) return;
-    const int l = q / g.NZ, k = q - l * g.NZ, i = blockIdx.y;
-    size_t n = g.node(i, l, k);
-    size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
-    if (i <= g.nx + 1 && l <= g.ny && k <= g.nz) Hx[n] += 0.5f * (cz * (Ey[n + 1] - Ey[n]) - cy * (Ez[n + sy] - Ez[n]));
-    if (i <= g.nx && l <= g.ny + 1 && k <= g.nz) Hy[n] += 0.5f * (cx * (Ez[n + sx] - Ez[n]) - cz * (Ex[n + 1] - Ex[n]));
-    if (i <= g.nx && l <= g.ny && k <= g.nz + 1) Hz[n] += 0.5f * (cy * (Ex[n + sy] - Ex[n]) - cx * (Ey[n + sx] - Ey[n]));
+    if (q >= g.NY * nq) return;
+    const int l = q / nq, k0 = (q - l * nq) * 4, i = blockIdx.y;
+    const size_t n = g.node(i, l, k0);
+    const size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
+    float ex[5], ey[5], ez[4], hx[4], hy[4], hz[4], ezy[4] = {}, exy[4] = {}, ezx[4] = {}, eyx[4] = {};
+    un4(ld4(Ex + n), ex); un4(ld4(Ey + n), ey); un4(ld4(Ez + n), ez);
+    un4(ld4(Hx + n), hx); un4(ld4(Hy + n), hy); un4(ld4(Hz + n), hz);
+    ex[4] = k0 + 4 < g.NZ ? Ex[n + 4] : 0.f;  // +z neighbour of the last node
+    ey[4] = k0 + 4 < g.NZ ? Ey[n + 4] : 0.f;
+    if (l + 1 < g.NY) { un4(ld4(Ez + n + sy), ezy); un4(ld4(Ex + n + sy), exy); }
+    if (i + 1 < g.NX) { un4(ld4(Ez + n + sx), ezx); un4(ld4(Ey + n + sx), eyx); }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int k = k0 + j;
+        if (i <= g.nx + 1 && l <= g.ny && k <= g.nz) {
+            const float q = q_half(cz, ey[j + 1], ey[j], cy, ezy[j], ez[j]);
+            hx[j] = __fadd_rn(hx[j], q);
+            if (TWICE) hx[j] = __fadd_rn(hx[j], q);
+        }
+        if (i <= g.nx && l <= g.ny + 1 && k <= g.nz) {
+            const float q = q_half(cx, ezx[j], ez[j], cz, ex[j + 1], ex[j]);
+            hy[j] = __fadd_rn(hy[j], q);
+            if (TWICE) hy[j] = __fadd_rn(hy[j], q);
+        }
+        if (i <= g.nx && l <= g.ny && k <= g.nz + 1) {
+            const float q = q_half(cy, exy[j], ex[j], cx, eyx[j], ey[j]);
+            hz[j] = __fadd_rn(hz[j], q);
+            if (TWICE) hz[j] = __fadd_rn(hz[j], q);
+        }
+    }
+    st4(Hx + n, hx); st4(Hy + n, hy); st4(Hz + n, hz);
 }
 
 // emeElement (kernels.cu:1091-1102) in FP32, tau*J formed in FP64
@@ -41,18 +91,36 @@ __global__ void k_e_update_mixed(Grid g, float *Ex, float *Ey, float *Ez, const 
                                  const float *__restrict__ Hy, const float *__restrict__ Hz,
                                  const double *__restrict__ Jx, const double *__restrict__ Jy,
                                  const double *__restrict__ Jz, float cx, float cy, float cz, double tau) {
-    // one thread per node of an x plane (l, k flattened: no idle z tail)
+    const int nq = g.pz / 4;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= g.NY * g.NZ) return;
-    const int l = q / g.NZ, k = q - l * g.NZ, i = blockIdx.y;
-    size_t n = g.node(i, l, k);
-    size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
-    if (i <= g.nx && l >= 1 && l <= g.ny && k >= 1 && k <= g.nz)
-        Ex[n] += cy * (Hz[n] - Hz[n - sy]) - cz * (Hy[n] - Hy[n - 1]) - (float)(tau * Jx[n]);
-    if (i >= 1 && i <= g.nx && l <= g.ny && k >= 1 && k <= g.nz)
-        Ey[n] += cz * (Hx[n] - Hx[n - 1]) - cx * (Hz[n] - Hz[n - sx]) - (float)(tau * Jy[n]);
-    if (i >= 1 && i <= g.nx && l >= 1 && l <= g.ny && k <= g.nz)
-        Ez[n] += cx * (Hy[n] - Hy[n - sx]) - cy * (Hx[n] - Hx[n - sy]) - (float)(tau * Jz[n]);
+    if (q >= g.NY * nq) return;
+    const int l = q / nq, k0 = (q - l * nq) * 4, i = blockIdx.y;
+    const size_t n = g.node(i, l, k0);
+    const size_t sx = (size_t)g.NY * g.pz, sy = g.pz;
+    float ex[4], ey[4], ez[4], hx[5], hy[5], hz[4], hzy[4] = {}, hxy[4] = {}, hzx[4] = {}, hyx[4] = {};
+    un4(ld4(Ex + n), ex); un4(ld4(Ey + n), ey); un4(ld4(Ez + n), ez);
+    // hx[0], hy[0]: the -z neighbour of the first node; hx[1..4]: the four nodes
+    un4(ld4(Hx + n), hx + 1); un4(ld4(Hy + n), hy + 1); un4(ld4(Hz + n), hz);
+    hx[0] = k0 > 0 ? Hx[n - 1] : 0.f;
+    hy[0] = k0 > 0 ? Hy[n - 1] : 0.f;
+    if (l >= 1) { un4(ld4(Hz + n - sy), hzy); un4(ld4(Hx + n - sy), hxy); }
+    if (i >= 1) { un4(ld4(Hz + n - sx), hzx); un4(ld4(Hy + n - sx), hyx); }
+    const double2 jx0 = *reinterpret_cast<const double2 *>(Jx + n), jx1 = *reinterpret_cast<const double2 *>(Jx + n + 2);
+    const double2 jy0 = *reinterpret_cast<const double2 *>(Jy + n), jy1 = *reinterpret_cast<const double2 *>(Jy + n + 2);
+    const double2 jz0 = *reinterpret_cast<const double2 *>(Jz + n), jz1 = *reinterpret_cast<const double2 *>(Jz + n + 2);
+    const double jx[4] = {jx0.x, jx0.y, jx1.x, jx1.y}, jy[4] = {jy0.x, jy0.y, jy1.x, jy1.y},
+                 jz[4] = {jz0.x, jz0.y, jz1.x, jz1.y};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int k = k0 + j;
+        if (i <= g.nx && l >= 1 && l <= g.ny && k >= 1 && k <= g.nz)
+            ex[j] = e_step(ex[j], cy, hz[j], hzy[j], cz, hy[j + 1], hy[j], tau * jx[j]);
+        if (i >= 1 && i <= g.nx && l <= g.ny && k >= 1 && k <= g.nz)
+            ey[j] = e_step(ey[j], cz, hx[j + 1], hx[j], cx, hz[j], hzx[j], tau * jy[j]);
+        if (i >= 1 && i <= g.nx && l >= 1 && l <= g.ny && k <= g.nz)
+            ez[j] = e_step(ez[j], cx, hy[j + 1], hyx[j], cy, hx[j + 1], hxy[j], tau * jz[j]);
+    }
+    st4(Ex + n, ex); st4(Ey + n, ey); st4(Ez + n, ez);
 }
 
 // ------------------------------------------------------- particle push --
@@ -276,15 +344,20 @@ __device__ __forceinline__ long long rescale(long long w, int sh) {
 
 // shared-memory layout of k_push_mixed (dynamic part), byte offsets
 struct MixedSmem {
-    size_t raw, raw_comp, quads, jw, tilej, holes, total;
+    size_t raw, raw_e, raw_h, quads, jw, tilej, holes, total;
+    // byte offset of component f (Ex Ey Ez Hx Hy Hz) in the raw staging area
+    __host__ __device__ size_t raw_of(int f) const { return raw + (f < 3 ? f * raw_e : 3 * raw_e + (f - 3) * raw_h); }
 };
 __host__ __device__ inline size_t round_up_sz(size_t v, size_t a) { return (v + a - 1) / a * a; }
 __host__ __device__ inline MixedSmem mixed_smem(int tx, int ty, int tz) {
     MixedSmem m;
     const size_t SX = tx + 2, SY = ty + 2, SZ = tz + 2, nn = SX * SY * SZ;
-    const size_t box = (size_t)(tx + 2) * (ty + 3) * (tz + 4);  // TMA box of one component
-    m.raw_comp = round_up_sz(box * sizeof(float), 128);
-    const size_t raw_bytes = 6 * m.raw_comp;
+    // TMA boxes: the tile + halo plus one row in y and two in z for the quads;
+    // E has one more x plane for the forward differences of the B half step
+    const size_t box_e = (size_t)(tx + 3) * (ty + 3) * (tz + 4), box_h = (size_t)(tx + 2) * (ty + 3) * (tz + 4);
+    m.raw_e = round_up_sz(box_e * sizeof(float), 128);
+    m.raw_h = round_up_sz(box_h * sizeof(float), 128);
+    const size_t raw_bytes = 3 * m.raw_e + 3 * m.raw_h;
     const size_t jw_bytes = (size_t)kJCopies * 3 * nn * sizeof(int);
     // the raw TMA staging area is consumed (into the quads) before the int32
     // currents are cleared, so the two share memory
@@ -356,11 +429,11 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned comp_bytes = (unsigned)((size_t)SX * BY * BZ * sizeof(float));
-        mbar_arrive_expect_tx(&sBar, 6 * comp_bytes);
+        const unsigned e_bytes = (unsigned)((size_t)(SX + 1) * BY * BZ * sizeof(float));
+        const unsigned h_bytes = (unsigned)((size_t)SX * BY * BZ * sizeof(float));
+        mbar_arrive_expect_tx(&sBar, 3 * e_bytes + 3 * h_bytes);
 #pragma unroll
-        for (int f = 0; f < 6; f++)
-            tma_load_3d(smem_raw + L.raw + f * L.raw_comp, &maps.m[f], &sBar, k0, l0, i0);
+        for (int f = 0; f < 6; f++) tma_load_3d(smem_raw + L.raw_of(f), &maps.m[f], &sBar, k0, l0, i0);
     }
     for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) sJ[idx] = 0ull;
     bool staged = false;
@@ -370,12 +443,33 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
         if (threadIdx.x == 0) atomicOr(&P.st->flags, ST_TMA);
         return;
     }
-    // raw [a][b][c] (c fastest, extents SX, BY, BZ) -> yz-quads
+    if (P.b_half) {
+        // the B half step of the staged tile (pic_step leaves the full-step H
+        // in memory): H += Q(E) on its ranges, at the nodes the quads read
+        float *R[6];
+#pragma unroll
+        for (int f = 0; f < 6; f++) R[f] = (float *)(smem_raw + L.raw_of(f));
+        const float bcx = (float)(g.tau / g.hx), bcy = (float)(g.tau / g.hy), bcz = (float)(g.tau / g.hz);
+        const int sbx = BY * BZ;  // x stride of the raw boxes
+        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+            const int a = idx / SYZ, bc = idx - a * SYZ, b = bc / SZ, c = bc - b * SZ;
+            const int gi = i0 + a, gl = l0 + b, gk = k0 + c;
+            const int o = (a * BY + b) * BZ + c;
+            if (gi <= g.nx + 1 && gl <= g.ny && gk <= g.nz)
+                R[3][o] = __fadd_rn(R[3][o], q_half(bcz, R[1][o + 1], R[1][o], bcy, R[2][o + BZ], R[2][o]));
+            if (gi <= g.nx && gl <= g.ny + 1 && gk <= g.nz)
+                R[4][o] = __fadd_rn(R[4][o], q_half(bcx, R[2][o + sbx], R[2][o], bcz, R[0][o + 1], R[0][o]));
+            if (gi <= g.nx && gl <= g.ny && gk <= g.nz + 1)
+                R[5][o] = __fadd_rn(R[5][o], q_half(bcy, R[0][o + BZ], R[0][o], bcx, R[1][o + sbx], R[1][o]));
+        }
+        __syncthreads();
+    }
+    // raw [a][b][c] (c fastest, extents SX (+1 for E), BY, BZ) -> yz-quads
     // Q[n] = (T[n], T[n+dz], T[n+dy], T[n+dy+dz]); out-of-array taps arrive as 0
     for (int idx = threadIdx.x; idx < 6 * nn; idx += blockDim.x) {
         const int f = idx / nn, r = idx - f * nn;
         const int a = r / SYZ, bc = r - a * SYZ, b = bc / SZ, c = bc - b * SZ;
-        const float *R = (const float *)(smem_raw + L.raw + f * L.raw_comp) + (a * BY + b) * BZ + c;
+        const float *R = (const float *)(smem_raw + L.raw_of(f)) + (a * BY + b) * BZ + c;
         sF[idx] = make_float4(R[0], R[1], R[BZ], R[BZ + 1]);
     }
     __syncthreads();
@@ -759,13 +853,19 @@ cudaError_t contribution_bound_mixed(const Grid &g, const SpeciesView &S, int64_
 }
 
 constexpr int kPlaneThreads = 256;
+// one thread per four z nodes of an x plane
 static inline dim3 plane_grid(const Grid &g) {
-    return dim3((g.NY * g.NZ + kPlaneThreads - 1) / kPlaneThreads, g.NX);
+    return dim3((g.NY * (g.pz / 4) + kPlaneThreads - 1) / kPlaneThreads, g.NX);
 }
 
 void yee_b_half_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s) {
     float cx = (float)(g.tau / g.hx), cy = (float)(g.tau / g.hy), cz = (float)(g.tau / g.hz);
-    k_b_half_mixed<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], cx, cy, cz);
+    k_b_half_mixed<false><<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], cx, cy, cz);
+}
+
+void yee_b_both_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s) {
+    float cx = (float)(g.tau / g.hx), cy = (float)(g.tau / g.hy), cz = (float)(g.tau / g.hz);
+    k_b_half_mixed<true><<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], cx, cy, cz);
 }
 
 void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], double *const J[3], cudaStream_t s) {
@@ -797,12 +897,15 @@ cudaError_t encode_field_maps(const Grid &g, float *const E[3], float *const H[3
     // a 16-byte boundary
     const cuuint64_t dims[3] = {(cuuint64_t)g.NZ, (cuuint64_t)g.NY, (cuuint64_t)g.NX};
     const cuuint64_t strides[2] = {(cuuint64_t)g.pz * sizeof(float), (cuuint64_t)g.pz * g.NY * sizeof(float)};
-    const cuuint32_t box[3] = {(cuuint32_t)(g.tz + 4), (cuuint32_t)(g.ty + 3), (cuuint32_t)(g.tx + 2)};
+    // E has one more x plane (the forward differences of the B half step)
+    const cuuint32_t box_e[3] = {(cuuint32_t)(g.tz + 4), (cuuint32_t)(g.ty + 3), (cuuint32_t)(g.tx + 3)};
+    const cuuint32_t box_h[3] = {(cuuint32_t)(g.tz + 4), (cuuint32_t)(g.ty + 3), (cuuint32_t)(g.tx + 2)};
     const cuuint32_t estr[3] = {1, 1, 1};
-    if (g.tz % 4 != 0 || box[0] > 256 || box[1] > 256 || box[2] > 256) return cudaErrorInvalidValue;
+    if (g.tz % 4 != 0 || box_e[0] > 256 || box_e[1] > 256 || box_e[2] > 256) return cudaErrorInvalidValue;
     float *const src[6] = {E[0], E[1], E[2], H[0], H[1], H[2]};
     for (int f = 0; f < 6; f++) {
-        CUresult r = encode(&maps->m[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)src[f], dims, strides, box, estr,
+        CUresult r = encode(&maps->m[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)src[f], dims, strides,
+                            f < 3 ? box_e : box_h, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
