@@ -334,6 +334,7 @@ constexpr int kMixedThreads = PIC_MIXED_THREADS;  // threads per CTA of k_push_m
 constexpr int kMixedWarps = kMixedThreads / 32;
 constexpr int kJCopies = kMixedWarps / 2;         // int32 tile currents per CTA: one per two warps
 constexpr int kQueue = PIC_MIXED_QUEUE;           // queued segments per warp
+constexpr unsigned kOutChunk = 16;                // outbox slots a warp takes from the global counter at once
 static_assert(kMixedThreads % 32 == 0, "whole warps");
 static_assert(kQueue >= 64, "one iteration can queue two segments per lane");
 
@@ -491,6 +492,10 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     double kin = 0.0;
     unsigned long long moved = 0;
     OutMixed *outbox = (OutMixed *)P.outbox;
+    // this warp's current outbox chunk [ob_base, ob_base + kOutChunk), ob_used
+    // slots taken (warp-uniform); chunks come from the global counter
+    unsigned ob_base = 0, ob_used = kOutChunk;
+    bool ob_any = false;
 
     for (int s = 0; s < P.nsp; s++) {
         const SpeciesView &S = P.sp[s];
@@ -716,26 +721,39 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
                 S.ox[slot] = xw[0]; S.oy[slot] = xw[1]; S.oz[slot] = xw[2];
                 S.fx[slot] = pu; S.fy[slot] = pv; S.fz[slot] = pw;
             }
-            // leavers: one outbox and one hole-list reservation per warp
+            // leavers: outbox slots from the warp's chunk (a new run of chunks
+            // from the global counter only when it is used up) and one
+            // hole-list reservation per warp
             const bool leave = active && !stay;
             const unsigned lm = __ballot_sync(FULL, leave);
             if (lm) {
                 const int nl = __popc(lm), rank = __popc(lm & lt);
-                unsigned obase = 0;
                 int hbase = 0;
-                if (lane == 0) {
-                    obase = atomicAdd(&P.st->out_count, (unsigned)nl);
-                    hbase = atomicAdd(&sNHoles[sp], nl);
-                }
-                obase = __shfl_sync(FULL, obase, 0);
+                if (lane == 0) hbase = atomicAdd(&sNHoles[sp], nl);
                 hbase = __shfl_sync(FULL, hbase, 0);
+                const unsigned room = kOutChunk - ob_used;
+                unsigned nb = 0;
+                if ((unsigned)nl > room) {
+                    const unsigned need = ((unsigned)nl - room + kOutChunk - 1) / kOutChunk;
+                    if (lane == 0) nb = atomicAdd(&P.st->out_count, need * kOutChunk);
+                    nb = __shfl_sync(FULL, nb, 0);
+                }
+                // leaver `rank` takes the room left in the chunk, then the new chunks
+                const unsigned e = (unsigned)rank < room ? ob_base + ob_used + rank : nb + (rank - room);
+                if ((unsigned)nl > room) {
+                    const unsigned over = (unsigned)nl - room;
+                    ob_base = nb + (over - 1) / kOutChunk * kOutChunk;
+                    ob_used = over - (over - 1) / kOutChunk * kOutChunk;
+                    ob_any = true;
+                } else {
+                    ob_used += nl;
+                }
                 if (leave) {
                     // the new cell, wrapped periodically
                     int ci[3] = {i + dl[0], l + dl[1], k + dl[2]};
                     const int nc[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
                     for (int d = 0; d < 3; d++) ci[d] = ci[d] == nc[d] ? 0 : (ci[d] < 0 ? nc[d] - 1 : ci[d]);
-                    const unsigned e = obase + rank;
                     if (e < P.out_cap) {
                         OutMixed o;
                         o.ox = xw[0]; o.oy = xw[1]; o.oz = xw[2]; o.px = pu; o.py = pv; o.pz = pw;
@@ -802,6 +820,9 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
     if (threadIdx.x < P.nsp && P.lb_cur && sLbMax[threadIdx.x]) atomicMax(&P.lb_cur[threadIdx.x], sLbMax[threadIdx.x]);
     __syncthreads();
 
+    // the unused slots of this warp's last outbox chunk: empty entries
+    if (ob_any && lane < kOutChunk - ob_used && ob_base + ob_used + lane < P.out_cap)
+        outbox[ob_base + ob_used + lane].cell = -1;
     for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
         long long iv = (long long)sJ[idx];
         if (iv != 0) {
