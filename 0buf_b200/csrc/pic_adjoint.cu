@@ -205,7 +205,7 @@ __device__ __forceinline__ void boris_plain(double q_m, double tau, const double
     pv += tau1 * F[1];
     pw += tau1 * F[2];
     B.u[0] = pu; B.u[1] = pv; B.u[2] = pw;
-    B.g1 = pow((pu * pu + pv * pv + pw * pw) * 1. + 1.0, -0.5);
+    B.g1 = 1.0 / sqrt((pu * pu + pv * pv + pw * pw) * 1. + 1.0);  // pow(v, -0.5), as in k_push_plain
     double ps = tau1 * B.g1;
     B.ps = ps;
     double bx = ps * F[3], by = ps * F[4], bz = ps * F[5];
@@ -225,7 +225,7 @@ __device__ __forceinline__ void boris_plain(double q_m, double tau, const double
     pv = pv1 + F[1] * tau1;
     pw = pw1 + F[2] * tau1;
     B.pp[0] = pu; B.pp[1] = pv; B.pp[2] = pw;
-    B.g2 = pow(((pu * pu + pv * pv + pw * pw) + 1.0), -0.5);
+    B.g2 = 1.0 / sqrt(((pu * pu + pv * pv + pw * pw) + 1.0));
     B.x1[0] = x[0] + tau * (B.g2 * pu);
     B.x1[1] = x[1] + tau * (B.g2 * pv);
     B.x1[2] = x[2] + tau * (B.g2 * pw);

@@ -85,6 +85,7 @@ void free_species(pic_handle *h, int s) {
     h->sp[s].cap_total = 0;
     h->sp[s].loaded = 0;
     h->sp[s].h_start.clear();
+    h->tile_cap_valid = 0;
 }
 
 // capacity per tile from counts; allocates the species arrays and uploads the
@@ -129,6 +130,7 @@ int alloc_species(pic_handle *h, int s, const std::vector<int> &counts) {
     h->sp[s].h_start = start;
     h->sp[s].loaded = 1;
     h->sp[s].lb_known = 0;
+    h->tile_cap_valid = 0;
     return PIC_OK;
 }
 
@@ -317,6 +319,29 @@ int do_b_half(pic_handle *h) {
     return PIC_OK;
 }
 
+// The plain push's int32 remainder word needs fewer than 2^(31 - kFxLo32MinBits)
+// particles in every tile.  A tile never holds more than its bins' capacities
+// (an overflow leaves the particle in the outbox and rebins), so the largest
+// per-tile sum of capacities over the species decides for the launch.
+bool plain_lo32(pic_handle *h) {
+    if (!h->tile_cap_valid) {
+        int64_t mx = 0;
+        for (int t = 0; t < h->g.ntiles; t++) {
+            int64_t c = 0;
+            for (int s = 0; s < h->cfg.nspecies; s++) {
+                const std::vector<int> &st = h->sp[s].h_start;
+                if (!st.empty()) c += st[t + 1] - st[t];
+            }
+            mx = std::max(mx, c);
+        }
+        h->tile_cap_max = mx;
+        h->tile_cap_valid = 1;
+    }
+    int b = 0;
+    while ((1ll << b) <= h->tile_cap_max) b++;
+    return 31 - b >= kFxLo32MinBits;
+}
+
 int do_push_deposit(pic_handle *h, int b_half_in_push = 0) {
     int rc = need_particles(h);
     if (rc) return rc;
@@ -340,7 +365,8 @@ int do_push_deposit(pic_handle *h, int b_half_in_push = 0) {
     StepParams p = make_params(h);
     p.b_half = b_half_in_push;
     cudaEventRecord(h->ev[2], h->stream);
-    CK(h->mixed ? launch_push_mixed(p, h->maps, h->stream) : launch_push_plain(p, h->stream), "push_deposit");
+    CK(h->mixed ? launch_push_mixed(p, h->maps, h->stream) : launch_push_plain(p, plain_lo32(h), h->stream),
+       "push_deposit");
     cudaEventRecord(h->ev[3], h->stream);
     if (h->mixed) h->lb_par ^= 1;
     h->launches += 1;

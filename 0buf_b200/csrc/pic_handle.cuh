@@ -64,6 +64,10 @@ struct pic_handle {
     pic::MixedMaps maps;
     float *lb_buf;
     int lb_par;
+    // plain form: the largest per-tile sum of bin capacities over the species
+    // (valid while tile_cap_valid; cleared whenever a species' bins change)
+    int tile_cap_valid;
+    int64_t tile_cap_max;
 };
 
 namespace pic_host {

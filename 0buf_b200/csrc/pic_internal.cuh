@@ -118,6 +118,31 @@ __device__ __forceinline__ void fx_add2(unsigned long long *hi, unsigned long lo
     if (ih) atomicAdd(hi, (unsigned long long)ih);
     if (il) atomicAdd(lo, (unsigned long long)il);
 }
+// The same split with an int32 second word (native 32-bit shared atomics: a
+// c2 FP64 push takes 22 ms less than with the 64-bit word).  The remainder
+// s - r (|s - r| <= 1/2) is counted in units of q * 2^-L, so one add is at
+// most 2^(L-1) in magnitude.  A tile of N particles adds at most 2N times to
+// one word (two zigzag segments per particle, one add per node of a segment),
+// so L = 31 - bits(N), N < 2^bits(N), keeps every sum below N 2^L < 2^31:
+// exact and order-independent like the 64-bit word, with |error| <=
+// q * 2^-(L+1) per contribution.  The push uses it when every tile's
+// capacity gives L >= kFxLo32MinBits (tiles below 2^17 particles; the
+// reference's default run, 2.6e5 particles per tile, keeps the 64-bit word).
+constexpr int kFxLo32MinBits = 14;
+__device__ __forceinline__ int fx_lo32_bits(long long n) {
+    int b = 0;
+    while ((1ll << b) <= n) b++;
+    return 31 - b;
+}
+__device__ __forceinline__ void fx_add_lo32(unsigned long long *hi, int *lo, double v, double inv_q,
+                                            double lo_scale) {
+    const double s = v * inv_q;
+    const double r = rint(s);
+    const long long ih = (long long)r;
+    const int il = __double2int_rn((s - r) * lo_scale);  // lo_scale = 2^L: exact
+    if (ih) atomicAdd(hi, (unsigned long long)ih);
+    if (il) atomicAdd(lo, il);
+}
 
 struct SpeciesView {
     // plain form

@@ -13,7 +13,9 @@ void j_fold(const Grid &g, double *Jx, double *Jy, double *Jz, cudaStream_t s);
 void e_ghosts_plain(const Grid &g, double *Ex, double *Ey, double *Ez, int periodic, cudaStream_t s);
 void e_ghosts_mixed(const Grid &g, float *Ex, float *Ey, float *Ez, int periodic, cudaStream_t s);
 size_t push_smem_plain(const Grid &g);
-cudaError_t launch_push_plain(const StepParams &p, cudaStream_t s);
+// lo32: the tile current's int32 remainder word (every tile holds fewer than
+// 2^(31 - kFxLo32MinBits) particles), else the 64-bit one
+cudaError_t launch_push_plain(const StepParams &p, bool lo32, cudaStream_t s);
 // placement of loaded particles (reference getPointCell + Cell::Insert)
 cudaError_t place_particles_plain(const Grid &g, int64_t n, const double *x, const double *y, const double *z,
                                   int *cell_out, cudaStream_t s);

@@ -165,38 +165,50 @@ __device__ __forceinline__ double interp_plain(const double *__restrict__ T, int
     return t2 + t1;
 }
 
-// pqr, cell.h:1511-1693, accumulating into the tile J (shared memory)
-__device__ __forceinline__ void pqr_plain(unsigned long long *__restrict__ sJ, double inv_q, int nn, int SY, int SZ,
-                                          int bi, int bl, int bk, const int iv[3], const double x[3],
-                                          const double x1[3], double a1, double hx, double hy, double hz, double tau,
-                                          double x0, double y0, double z0, unsigned &bad) {
+// pqr, cell.h:1511-1693, accumulating into the tile J (shared memory).  The
+// reference's divisions by 12 and by tau*h*h are multiplications by their
+// reciprocals (rc[d] = 1 / (tau * h_e * h_f), precomputed): the products feed
+// only the current's magnitude, never an index, and differ from the quotients
+// by an ulp.  LO32 selects the int32 remainder word (fx_add_lo32; words at
+// sJ + 3 nn as 3 nn ints), else the 64-bit one (fx_add2; 3 nn words).
+template <bool LO32>
+__device__ __forceinline__ void pqr_plain(unsigned long long *__restrict__ sJ, double inv_q, double lo_scale, int nn,
+                                          int SY, int SZ, int bi, int bl, int bk, const int iv[3], const double x[3],
+                                          const double x1[3], double a1, double hx, double hy, double hz,
+                                          const double rc[3], double x0, double y0, double z0, unsigned &bad) {
     double dx = (0.50 * (x[0] + x1[0]) - hx * ((double)iv[0] - 2.50) - x0);
     double dy = (0.50 * (x[1] + x1[1]) - hy * ((double)iv[1] - 2.50) - y0);
     double dz = (0.50 * (x[2] + x1[2]) - hz * ((double)iv[2] - 2.50) - z0);
     double a = a1;
     double dx1 = hx - dx, dy1 = hy - dy, dz1 = hz - dz;
     double su = x1[0] - x[0], sv = x1[1] - x[1], sw = x1[2] - x[2];
-    double s1 = sv * sw / 12.0, s2 = su * sw / 12.0, s3 = su * sv / 12.0;
-    su = su * a / (tau * hy * hz);
-    sv = sv * a / (tau * hx * hz);
-    sw = sw * a / (tau * hx * hy);
+    constexpr double kTwelfth = 1.0 / 12.0;
+    double s1 = sv * sw * kTwelfth, s2 = su * sw * kTwelfth, s3 = su * sv * kTwelfth;
+    su = su * a * rc[0];
+    sv = sv * a * rc[1];
+    sw = sw * a * rc[2];
     if (iv[0] < 2 || iv[0] > 3 || iv[1] < 2 || iv[1] > 3 || iv[2] < 2 || iv[2] > 3) { bad |= ST_STENCIL; return; }
-    int n = ((bi + iv[0]) * SY + (bl + iv[1])) * SZ + (bk + iv[2]);
-    int ez = 1, ey = SZ, ex = SY * SZ;
-    unsigned long long *Jx = sJ, *Jy = sJ + nn, *Jz = sJ + 2 * nn;  // low words at + 3 nn
-    const int lo = 3 * nn;
-    fx_add2(&Jx[n], &Jx[n + lo], su * (dy1 * dz1 + s1), inv_q);
-    fx_add2(&Jx[n + ez], &Jx[n + ez + lo], su * (dy1 * dz - s1), inv_q);
-    fx_add2(&Jx[n + ey], &Jx[n + ey + lo], su * (dy * dz1 - s1), inv_q);
-    fx_add2(&Jx[n + ey + ez], &Jx[n + ey + ez + lo], su * (dy * dz + s1), inv_q);
-    fx_add2(&Jy[n], &Jy[n + lo], sv * (dx1 * dz1 + s2), inv_q);
-    fx_add2(&Jy[n + ez], &Jy[n + ez + lo], sv * (dx1 * dz - s2), inv_q);
-    fx_add2(&Jy[n + ex], &Jy[n + ex + lo], sv * (dx * dz1 - s2), inv_q);
-    fx_add2(&Jy[n + ex + ez], &Jy[n + ex + ez + lo], sv * (dx * dz + s2), inv_q);
-    fx_add2(&Jz[n], &Jz[n + lo], sw * (dx1 * dy1 + s3), inv_q);
-    fx_add2(&Jz[n + ey], &Jz[n + ey + lo], sw * (dx1 * dy - s3), inv_q);
-    fx_add2(&Jz[n + ex], &Jz[n + ex + lo], sw * (dx * dy1 - s3), inv_q);
-    fx_add2(&Jz[n + ex + ey], &Jz[n + ex + ey + lo], sw * (dx * dy + s3), inv_q);
+    const int n = ((bi + iv[0]) * SY + (bl + iv[1])) * SZ + (bk + iv[2]);
+    const int ez = 1, ey = SZ, ex = SY * SZ;
+    int *lo32 = (int *)(sJ + 3 * nn);
+    // component c, node offset o from n
+    auto add = [&](int c, int o, double v) {
+        const int w = c * nn + n + o;
+        if (LO32) fx_add_lo32(&sJ[w], &lo32[w], v, inv_q, lo_scale);
+        else fx_add2(&sJ[w], &sJ[3 * nn + w], v, inv_q);
+    };
+    add(0, 0, su * (dy1 * dz1 + s1));
+    add(0, ez, su * (dy1 * dz - s1));
+    add(0, ey, su * (dy * dz1 - s1));
+    add(0, ey + ez, su * (dy * dz + s1));
+    add(1, 0, sv * (dx1 * dz1 + s2));
+    add(1, ez, sv * (dx1 * dz - s2));
+    add(1, ex, sv * (dx * dz1 - s2));
+    add(1, ex + ez, sv * (dx * dz + s2));
+    add(2, 0, sw * (dx1 * dy1 + s3));
+    add(2, ey, sw * (dx1 * dy - s3));
+    add(2, ex, sw * (dx * dy1 - s3));
+    add(2, ex + ey, sw * (dx * dy + s3));
 }
 
 // Reflect, cell.h:1427-1478
@@ -237,11 +249,12 @@ static_assert(kPlainThreads % 32 == 0, "whole warps");
 #else
 #define PIC_PLAIN_BOUNDS __launch_bounds__(kPlainThreads)
 #endif
+template <bool LO32>
 __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int sNHoles, sNFront, sNMove;
     __shared__ double sRed[kPlainThreads / 32];
-    __shared__ double sQ, sInvQ;
+    __shared__ double sQ, sInvQ, sLoScale;
     const Grid &g = P.g;
     const int t = blockIdx.x;
     const int tk = t % g.ntz, tl = (t / g.ntz) % g.nty, ti = t / (g.ntz * g.nty);
@@ -249,16 +262,23 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
     const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
     const int nn = SX * SY * SZ;
     double *sF = (double *)smem_raw;  // Ex Ey Ez Hx Hy Hz
-    unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);  // fixed-point tile J: 3 nn high, 3 nn low words
+    // fixed-point tile J: 3 nn high words, then the remainder words (3 nn
+    // 64-bit, or 3 nn int32 in the first half of that space)
+    unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);
     int *sHoles = (int *)(sJ + 6 * nn);
     int *sFront = sHoles + kHoleMax;
     if (threadIdx.x == 0) {
         double bound = 0.0;
-        for (int s = 0; s < P.nsp; s++) bound += 2.5 * fabs(P.sp[s].m) * (double)P.sp[s].tile_count[t];
+        long long ntile = 0;
+        for (int s = 0; s < P.nsp; s++) {
+            bound += 2.5 * fabs(P.sp[s].m) * (double)P.sp[s].tile_count[t];
+            ntile += P.sp[s].tile_count[t];
+        }
         int e2;
         frexp(bound, &e2);  // bound < 2^e2
         sQ = ldexp(1.0, e2 - 62);
         sInvQ = ldexp(1.0, 62 - e2);
+        sLoScale = LO32 ? ldexp(1.0, fx_lo32_bits(ntile)) : 1099511627776.0;  // 2^L or 2^40
     }
 
     // stage E^n and H^{n+1/2} of nodes [i0, i0+tx+2) x [l0, ..) x [k0, ..)
@@ -281,7 +301,9 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
     __syncthreads();
 
     const double hx = g.hx, hy = g.hy, hz = g.hz, tau = g.tau;
-    const double inv_q = sInvQ;
+    const double inv_q = sInvQ, lo_scale = sLoScale;
+    // reciprocals of the reference's tau*h*h divisors in pqr
+    const double rc[3] = {1.0 / (tau * hy * hz), 1.0 / (tau * hx * hz), 1.0 / (tau * hx * hy)};
     unsigned bad = 0;
     double kin = 0.0;
     unsigned long long moved = 0, dropped = 0, dup = 0;
@@ -340,22 +362,28 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
             pu += tau1 * fEx;
             pv += tau1 * fEy;
             pw += tau1 * fEz;
-            double ps = tau1 * pow((pu * pu + pv * pv + pw * pw) * 1. + 1.0, -0.5);
+            // pow(v, -0.5) of the reference as 1 / sqrt(v): two correctly rounded
+            // operations, within an ulp of the reference's pow and without its
+            // logarithm/exponential code (16 ms of a c2 push)
+            double ps = tau1 * (1.0 / sqrt((pu * pu + pv * pv + pw * pw) * 1. + 1.0));
             {
                 double bx = ps * fHx, by = ps * fHy, bz = ps * fHz;
                 double su = pu + pv * bz - pw * by;
                 double sv = pv + pw * bx - pu * bz;
                 double sw = pw + pu * by - pv * bx;
                 double q1 = bx * bx, q2 = by * by, q3 = bz * bz, q4 = bx * by, q5 = by * bz, q6 = bz * bx;
+                // the reference's three divisions by sd as one reciprocal
+                // (continuous values only: within an ulp of the quotients)
                 double sd = q1 + 1. + q2 + q3;
-                double pu1 = ((q1 + 1.) * su + (q4 + bz) * sv + (q6 - by) * sw) / sd;
-                double pv1 = ((q4 - bz) * su + (q2 + 1.) * sv + (q5 + bx) * sw) / sd;
-                double pw1 = ((q6 + by) * su + (q5 - bx) * sv + (q3 + 1.) * sw) / sd;
+                const double isd = 1.0 / sd;
+                double pu1 = ((q1 + 1.) * su + (q4 + bz) * sv + (q6 - by) * sw) * isd;
+                double pv1 = ((q4 - bz) * su + (q2 + 1.) * sv + (q5 + bx) * sw) * isd;
+                double pw1 = ((q6 + by) * su + (q5 - bx) * sv + (q3 + 1.) * sw) * isd;
                 pu = pu1 + fEx * tau1;
                 pv = pv1 + fEy * tau1;
                 pw = pw1 + fEz * tau1;
             }
-            ps = pow(((pu * pu + pv * pv + pw * pw) + 1.0), -0.5);
+            ps = 1.0 / sqrt(((pu * pu + pv * pv + pw * pw) + 1.0));
             double xn[3] = {x + tau * (ps * pu), y + tau * (ps * pv), z + tau * (ps * pw)};
             if (!(isfinite(pu) && isfinite(pv) && isfinite(pw))) bad |= ST_NAN;
             {
@@ -408,11 +436,22 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
 #undef PROD
 #undef RBX
 #undef SQ
-                if (m >= 1 && m <= 7) {
-                    pqr_plain(sJ, inv_q, nn, SY, SZ, bi, bl, bk, i1, xo, x2, mw, hx, hy, hz, tau, x0, y0, z0, bad);
-                    pqr_plain(sJ, inv_q, nn, SY, SZ, bi, bl, bk, i2, x2, xn, mw, hx, hy, hz, tau, x0, y0, z0, bad);
-                } else {
-                    pqr_plain(sJ, inv_q, nn, SY, SZ, bi, bl, bk, i1, xo, xn, mw, hx, hy, hz, tau, x0, y0, z0, bad);
+                // one segment (xo -> xn) without a crossing, else xo -> x2 -> xn;
+                // one copy of pqr in the loop body keeps the kernel's code small
+                // (the front end starved on three inlined copies)
+                const int nseg = (m >= 1 && m <= 7) ? 2 : 1;
+#pragma unroll 1
+                for (int sg = 0; sg < nseg; sg++) {
+                    int iv[3];
+                    double sa[3], sb[3];
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        iv[d] = sg ? i2[d] : i1[d];
+                        sa[d] = sg ? x2[d] : xo[d];
+                        sb[d] = (nseg == 2 && sg == 0) ? x2[d] : xn[d];
+                    }
+                    pqr_plain<LO32>(sJ, inv_q, lo_scale, nn, SY, SZ, bi, bl, bk, iv, sa, sb, mw, hx, hy, hz, rc, x0,
+                                    y0, z0, bad);
                 }
             }
             x = reflect_plain(xn[0], g.lx);
@@ -498,13 +537,14 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
 
     // ---- tile J -> global J (GPU_WriteAllCurrents, kernels.cu:83-112)
     for (int idx = threadIdx.x; idx < 3 * nn; idx += blockDim.x) {
-        const long long ih = (long long)sJ[idx], il = (long long)sJ[3 * nn + idx];
+        const long long ih = (long long)sJ[idx];
+        const long long il = LO32 ? (long long)((const int *)(sJ + 3 * nn))[idx] : (long long)sJ[3 * nn + idx];
         if (ih != 0 || il != 0) {
             int comp = idx / nn, r = idx % nn;
             int c = r % SZ, b = (r / SZ) % SY, a = r / (SZ * SY);
             if (i0 + a < g.NX && l0 + b < g.NY && k0 + c < g.NZ)
                 atomicAdd(&P.J[comp][g.node(i0 + a, l0 + b, k0 + c)],
-                          ((double)ih + (double)il * 9.094947017729282e-13) * sQ);  // il * 2^-40
+                          ((double)ih + (double)il / lo_scale) * sQ);  // exact scale: a power of two
         }
     }
     // ---- kinetic energy and counters
@@ -595,11 +635,12 @@ size_t push_smem_plain(const Grid &g) {
     return 6 * nn * sizeof(double) + 6 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
 }
 
-cudaError_t launch_push_plain(const StepParams &p, cudaStream_t s) {
+cudaError_t launch_push_plain(const StepParams &p, bool lo32, cudaStream_t s) {
     size_t smem = push_smem_plain(p.g);
-    cudaError_t e = cudaFuncSetAttribute(k_push_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto *kern = lo32 ? k_push_plain<true> : k_push_plain<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_push_plain<<<p.g.ntiles, kPlainThreads, smem, s>>>(p);
+    kern<<<p.g.ntiles, kPlainThreads, smem, s>>>(p);
     return cudaGetLastError();
 }
 
