@@ -232,10 +232,11 @@ __device__ __forceinline__ int receivers(double x, int c, int N, double h, int o
 }
 
 // 512 threads, two CTAs per SM: 32 warps per SM at 64 registers (ptxas
-// spills ~200 bytes).  The kernel waits on shared-atomic round trips and FP64
+// spills ~300 bytes).  The kernel waits on shared-atomic round trips and FP64
 // dependency chains, and the extra warps hide them: c2 push 208.7 ms against
 // 246.5 ms with 256 threads at 126 registers (320: 229.8, 384: 219.8,
-// 448: 214.5, 256 x 3 CTAs: 218.4)
+// 448: 214.5, 256 x 3 CTAs: 218.4); with one pqr call site, 163.3 ms against
+// 189.4 at 384 threads
 #ifndef PIC_PLAIN_THREADS
 #define PIC_PLAIN_THREADS 512
 #endif

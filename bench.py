@@ -47,7 +47,10 @@ BYTES_PER_CELL_UPDATE = {"fp32": 72, "fp64": 120}
 # profiles/push_mixed_128x64x64_ncu.md (2.820 GB) and
 # profiles/push_plain_128x64x64_ncu.md (5.271 GB)
 NCU_TRAFFIC_PER_PARTICLE = {"fp32": 2.820e9 / 50331648, "fp64": 5.271e9 / 50331648}
-KERNELS_PER_STEP_NOTE = "b_half, push, insert, clamp, j_fold x3, b_complete, e_update, e_ghosts x2"
+KERNELS_PER_STEP_NOTE = {
+    "fp32": "push (forms the B half step of its staged tile), insert, clamp, j_fold x3, b_half twice in one pass, "
+            "e_update, e_ghosts x2; plus k_contribution_bound once per species after a load",
+    "fp64": "b_half, push, insert, clamp, j_fold x3, b_complete, e_update, e_ghosts x2"}
 
 
 def peaks():
@@ -260,7 +263,7 @@ def run_ours(args, dist):
         "yee": yee,
         "phases_ms": {k: round(statistics.mean(v), 4) for k, v in phases.items()},
         "gpu_launches": launches,
-        "launches_note": KERNELS_PER_STEP_NOTE,
+        "launches_note": KERNELS_PER_STEP_NOTE[form],
         "energy_after": energy_last,
     }
     if clocks:
