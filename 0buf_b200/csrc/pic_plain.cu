@@ -244,6 +244,9 @@ __device__ __forceinline__ int receivers(double x, int c, int N, double h, int o
 #define PIC_PLAIN_MIN_BLOCKS 2
 #endif
 constexpr int kPlainThreads = PIC_PLAIN_THREADS;  // threads per CTA of k_push_plain
+// per-warp queue of second zigzag segments: drained when it holds 16 or more
+// (at most 32 per drain), so it never holds more than 15 + 32 entries
+constexpr int kQPlain = 48;
 static_assert(kPlainThreads % 32 == 0, "whole warps");
 #ifdef PIC_PLAIN_MIN_BLOCKS
 #define PIC_PLAIN_BOUNDS __launch_bounds__(kPlainThreads, PIC_PLAIN_MIN_BLOCKS)
@@ -256,8 +259,10 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
     __shared__ int sNHoles, sNFront, sNMove;
     __shared__ double sRed[kPlainThreads / 32];
     __shared__ double sQ, sInvQ, sLoScale;
+    __shared__ int sQn[kPlainThreads / 32];  // entries in each warp's segment queue
     const Grid &g = P.g;
     const int t = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tk = t % g.ntz, tl = (t / g.ntz) % g.nty, ti = t / (g.ntz * g.nty);
     const int i0 = ti * g.tx, l0 = tl * g.ty, k0 = tk * g.tz;
     const int SX = g.tx + 2, SY = g.ty + 2, SZ = g.tz + 2;
@@ -268,6 +273,10 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
     unsigned long long *sJ = (unsigned long long *)(sF + 6 * nn);
     int *sHoles = (int *)(sJ + 6 * nn);
     int *sFront = sHoles + kHoleMax;
+    // this warp's segment queue: x2 and xn (6 x kQPlain doubles), and the
+    // start cell (tile-local) with the segment's centre-cell bits
+    double *qd = (double *)(sHoles + 2 * kHoleMax) + warp * 6 * kQPlain;
+    int *qc = (int *)((double *)(sHoles + 2 * kHoleMax) + (kPlainThreads / 32) * 6 * kQPlain) + warp * kQPlain;
     if (threadIdx.x == 0) {
         double bound = 0.0;
         long long ntile = 0;
@@ -317,198 +326,239 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
         const double q_m = S.q_m, mw = S.m, M = S.m / S.q_m;
         if (threadIdx.x == 0) { sNHoles = 0; sNFront = 0; sNMove = 0; }
         __syncthreads();
-        for (int j = threadIdx.x; j < count; j += blockDim.x) {
+        int qn = 0;  // entries in this warp's segment queue (warp-uniform)
+        if (lane == 0) sQn[warp] = 0;
+        __syncwarp();
+        // Whole warps iterate together (the queue is drained by whole warps),
+        // and past the last particle until the queue is empty.
+        for (int jw = threadIdx.x - lane;; jw += blockDim.x) {
+            const bool tail = jw >= count;
+            if (tail && qn == 0) break;
+            const int j = jw + lane;
             const int slot = start + j;
-            const int cell = S.cell[slot];
-            if (cell < 0) continue;  // dead slot left by an overflowed compaction
-            int i, l, k;
-            g.cell_ijk(cell, i, l, k);
+            // cell < 0: past the bin's end, or a dead slot left by an overflowed compaction
+            const int cell = (!tail && j < count) ? S.cell[slot] : -1;
+            int i = 0, l = 0, k = 0;
+            if (cell >= 0) g.cell_ijk(cell, i, l, k);
             const int bi = i - i0 - 2, bl = l - l0 - 2, bk = k - k0 - 2;
-            if (bi < -2 || bi >= g.tx - 2 || bl < -2 || bl >= g.ty - 2 || bk < -2 || bk >= g.tz - 2) {
-                bad |= ST_BADCELL;  // a bin entry outside its tile: never index the tile with it
-                continue;
-            }
-            // Cell ctor, cell.h:731-737
-            const double x0 = (double)i * hx, y0 = (double)l * hy, z0 = (double)k * hz;
-            double x = S.x[slot], y = S.y[slot], z = S.z[slot];
-            double pu = S.px[slot], pv = S.py[slot], pw = S.pz[slot];
+            const bool in_tile = bi >= -2 && bi < g.tx - 2 && bl >= -2 && bl < g.ty - 2 && bk >= -2 && bk < g.tz - 2;
+            if (cell >= 0 && !in_tile) bad |= ST_BADCELL;  // a bin entry outside its tile: never index the tile with it
+            if (cell >= 0 && in_tile) {
+                // Cell ctor, cell.h:731-737
+                const double x0 = (double)i * hx, y0 = (double)l * hy, z0 = (double)k * hz;
+                double x = S.x[slot], y = S.y[slot], z = S.z[slot];
+                double pu = S.px[slot], pv = S.py[slot], pw = S.pz[slot];
 
-            // ---- Cell::GetField, cell.h:1257-1290 (InverseKernel 1010-1047)
-            double fEx, fEy, fEz, fHx, fHy, fHz;
-            if (x < 0 || y < 0 || z < 0) {
-                fEx = fEy = fEz = fHx = fHy = fHz = 0.0;
-            } else {
-                int ix = (int)((x - x0) / hx + 1.0) + 1;
-                int i1x = (int)(((x - x0) / hx + 1.0) + 1.5);
-                double s1 = (int)(x / hx + 1.0) - x / hx;
-                double s2 = (int)(x / hx + 1.5) - 0.5 - x / hx;
-                int iy = (int)((y - y0) / hy + 1.0) + 1;
-                int i1y = (int)(((y - y0) / hy + 1.0) + 1.5);
-                double s3 = (int)(y / hy + 1.0) - y / hy;
-                double s4 = (int)(y / hy + 1.5) - 0.5 - y / hy;
-                int iz = (int)((z - z0) / hz + 1.0) + 1;
-                int i1z = (int)(((z - z0) / hz + 1.0) + 1.5);
-                double s5 = (int)(z / hz + 1.0) - z / hz;
-                double s6 = (int)(z / hz + 1.5) - 0.5 - z / hz;
-                double s11 = 1. - s1, s21 = 1. - s2, s31 = 1. - s3, s41 = 1. - s4, s51 = 1. - s5, s61 = 1. - s6;
-                fEx = interp_plain(sF, SY, SZ, bi, bl, bk, ix, i1y, i1z, s1, s11, s4, s41, s6, s61, bad);
-                fEy = interp_plain(sF + nn, SY, SZ, bi, bl, bk, i1x, iy, i1z, s2, s21, s3, s31, s6, s61, bad);
-                fEz = interp_plain(sF + 2 * nn, SY, SZ, bi, bl, bk, i1x, i1y, iz, s2, s21, s4, s41, s5, s51, bad);
-                fHx = interp_plain(sF + 3 * nn, SY, SZ, bi, bl, bk, i1x, iy, iz, s2, s21, s3, s31, s5, s51, bad);
-                fHy = interp_plain(sF + 4 * nn, SY, SZ, bi, bl, bk, ix, i1y, iz, s1, s11, s4, s41, s5, s51, bad);
-                fHz = interp_plain(sF + 5 * nn, SY, SZ, bi, bl, bk, ix, iy, i1z, s1, s11, s3, s31, s6, s61, bad);
-            }
-            // ---- Particle::Move, particle.h:65-202
-            double tau1 = q_m * tau * 0.5;
-            pu += tau1 * fEx;
-            pv += tau1 * fEy;
-            pw += tau1 * fEz;
-            // pow(v, -0.5) of the reference as 1 / sqrt(v): two correctly rounded
-            // operations, within an ulp of the reference's pow and without its
-            // logarithm/exponential code (16 ms of a c2 push)
-            double ps = tau1 * (1.0 / sqrt((pu * pu + pv * pv + pw * pw) * 1. + 1.0));
-            {
-                double bx = ps * fHx, by = ps * fHy, bz = ps * fHz;
-                double su = pu + pv * bz - pw * by;
-                double sv = pv + pw * bx - pu * bz;
-                double sw = pw + pu * by - pv * bx;
-                double q1 = bx * bx, q2 = by * by, q3 = bz * bz, q4 = bx * by, q5 = by * bz, q6 = bz * bx;
-                // the reference's three divisions by sd as one reciprocal
-                // (continuous values only: within an ulp of the quotients)
-                double sd = q1 + 1. + q2 + q3;
-                const double isd = 1.0 / sd;
-                double pu1 = ((q1 + 1.) * su + (q4 + bz) * sv + (q6 - by) * sw) * isd;
-                double pv1 = ((q4 - bz) * su + (q2 + 1.) * sv + (q5 + bx) * sw) * isd;
-                double pw1 = ((q6 + by) * su + (q5 - bx) * sv + (q3 + 1.) * sw) * isd;
-                pu = pu1 + fEx * tau1;
-                pv = pv1 + fEy * tau1;
-                pw = pw1 + fEz * tau1;
-            }
-            ps = 1.0 / sqrt(((pu * pu + pv * pv + pw * pw) + 1.0));
-            double xn[3] = {x + tau * (ps * pu), y + tau * (ps * pv), z + tau * (ps * pw)};
-            if (!(isfinite(pu) && isfinite(pv) && isfinite(pw))) bad |= ST_NAN;
-            {
-                double p2 = pu * pu + pv * pv + pw * pw;
-                kin += M * (p2 / (sqrt(1.0 + p2) + 1.0));  // gamma - 1 without cancellation
-            }
-
-            // ---- Cell::CurrentToMesh, cell.h:1306-1422
-            {
-                double xo[3] = {x, y, z}, x2[3] = {0.0, 0.0, 0.0}, sr;
-                const double h3[3] = {hx, hy, hz}, o3[3] = {x0, y0, z0};
-                int i1[3], i2[3];
-#pragma unroll
-                for (int d = 0; d < 3; d++) {  // getCellNumberCenterCurrent, cell.h:577-578
-                    double tt = ((xo[d] - o3[d]) / h3[d] + 1.5);
-                    i1[d] = (int)(tt + 1);
-                    double t2 = ((xn[d] - o3[d]) / h3[d] + 1.5);
-                    i2[d] = (int)(t2 + 1);
+                // ---- Cell::GetField, cell.h:1257-1290 (InverseKernel 1010-1047)
+                double fEx, fEy, fEz, fHx, fHy, fHz;
+                if (x < 0 || y < 0 || z < 0) {
+                    fEx = fEy = fEz = fHx = fHy = fHz = 0.0;
+                } else {
+                    int ix = (int)((x - x0) / hx + 1.0) + 1;
+                    int i1x = (int)(((x - x0) / hx + 1.0) + 1.5);
+                    double s1 = (int)(x / hx + 1.0) - x / hx;
+                    double s2 = (int)(x / hx + 1.5) - 0.5 - x / hx;
+                    int iy = (int)((y - y0) / hy + 1.0) + 1;
+                    int i1y = (int)(((y - y0) / hy + 1.0) + 1.5);
+                    double s3 = (int)(y / hy + 1.0) - y / hy;
+                    double s4 = (int)(y / hy + 1.5) - 0.5 - y / hy;
+                    int iz = (int)((z - z0) / hz + 1.0) + 1;
+                    int i1z = (int)(((z - z0) / hz + 1.0) + 1.5);
+                    double s5 = (int)(z / hz + 1.0) - z / hz;
+                    double s6 = (int)(z / hz + 1.5) - 0.5 - z / hz;
+                    double s11 = 1. - s1, s21 = 1. - s2, s31 = 1. - s3, s41 = 1. - s4, s51 = 1. - s5, s61 = 1. - s6;
+                    fEx = interp_plain(sF, SY, SZ, bi, bl, bk, ix, i1y, i1z, s1, s11, s4, s41, s6, s61, bad);
+                    fEy = interp_plain(sF + nn, SY, SZ, bi, bl, bk, i1x, iy, i1z, s2, s21, s3, s31, s6, s61, bad);
+                    fEz = interp_plain(sF + 2 * nn, SY, SZ, bi, bl, bk, i1x, i1y, iz, s2, s21, s4, s41, s5, s51, bad);
+                    fHx = interp_plain(sF + 3 * nn, SY, SZ, bi, bl, bk, i1x, iy, iz, s2, s21, s3, s31, s5, s51, bad);
+                    fHy = interp_plain(sF + 4 * nn, SY, SZ, bi, bl, bk, ix, i1y, iz, s1, s11, s4, s41, s5, s51, bad);
+                    fHz = interp_plain(sF + 5 * nn, SY, SZ, bi, bl, bk, ix, iy, i1z, s1, s11, s3, s31, s6, s61, bad);
                 }
-                int m = 4 * abs(i2[0] - i1[0]) + 2 * abs(i2[1] - i1[1]) + abs(i2[2] - i1[2]);
+                // ---- Particle::Move, particle.h:65-202
+                double tau1 = q_m * tau * 0.5;
+                pu += tau1 * fEx;
+                pv += tau1 * fEy;
+                pw += tau1 * fEz;
+                // pow(v, -0.5) of the reference as 1 / sqrt(v): two correctly rounded
+                // operations, within an ulp of the reference's pow and without its
+                // logarithm/exponential code (16 ms of a c2 push)
+                double ps = tau1 * (1.0 / sqrt((pu * pu + pv * pv + pw * pw) * 1. + 1.0));
+                {
+                    double bx = ps * fHx, by = ps * fHy, bz = ps * fHz;
+                    double su = pu + pv * bz - pw * by;
+                    double sv = pv + pw * bx - pu * bz;
+                    double sw = pw + pu * by - pv * bx;
+                    double q1 = bx * bx, q2 = by * by, q3 = bz * bz, q4 = bx * by, q5 = by * bz, q6 = bz * bx;
+                    // the reference's three divisions by sd as one reciprocal
+                    // (continuous values only: within an ulp of the quotients)
+                    double sd = q1 + 1. + q2 + q3;
+                    const double isd = 1.0 / sd;
+                    double pu1 = ((q1 + 1.) * su + (q4 + bz) * sv + (q6 - by) * sw) * isd;
+                    double pv1 = ((q4 - bz) * su + (q2 + 1.) * sv + (q5 + bx) * sw) * isd;
+                    double pw1 = ((q6 + by) * su + (q5 - bx) * sv + (q3 + 1.) * sw) * isd;
+                    pu = pu1 + fEx * tau1;
+                    pv = pv1 + fEy * tau1;
+                    pw = pw1 + fEz * tau1;
+                }
+                ps = 1.0 / sqrt(((pu * pu + pv * pv + pw * pw) + 1.0));
+                double xn[3] = {x + tau * (ps * pu), y + tau * (ps * pv), z + tau * (ps * pw)};
+                if (!(isfinite(pu) && isfinite(pv) && isfinite(pw))) bad |= ST_NAN;
+                {
+                    double p2 = pu * pu + pv * pv + pw * pw;
+                    kin += M * (p2 / (sqrt(1.0 + p2) + 1.0));  // gamma - 1 without cancellation
+                }
+
+                // ---- Cell::CurrentToMesh, cell.h:1306-1422
+                {
+                    double xo[3] = {x, y, z}, x2[3] = {0.0, 0.0, 0.0}, sr;
+                    const double h3[3] = {hx, hy, hz}, o3[3] = {x0, y0, z0};
+                    int i1[3], i2[3];
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {  // getCellNumberCenterCurrent, cell.h:577-578
+                        double tt = ((xo[d] - o3[d]) / h3[d] + 1.5);
+                        i1[d] = (int)(tt + 1);
+                        double t2 = ((xn[d] - o3[d]) / h3[d] + 1.5);
+                        i2[d] = (int)(t2 + 1);
+                    }
+                    int m = 4 * abs(i2[0] - i1[0]) + 2 * abs(i2[1] - i1[1]) + abs(i2[2] - i1[2]);
 #define AVG(d) (h3[d] * (((double)i1[d] + (double)i2[d]) * 0.5 - 2.0) + o3[d])
 #define RATIO(d) ((x2[d] - xo[d]) / (xn[d] - xo[d]))
 #define PROD(d) ((x2[d] - xo[d]) * (xn[d] - xo[d]))
 #define RBX(d) (xo[d] + (xn[d] - xo[d]) * sr)
 #define SQ(v) ((v) * (v))
-                switch (m) {
-                    case 1: x2[2] = AVG(2); sr = RATIO(2); x2[0] = RBX(0); x2[1] = RBX(1); break;
-                    case 2: x2[1] = AVG(1); sr = RATIO(1); x2[0] = RBX(0); x2[2] = RBX(2); break;
-                    case 3:
-                        x2[1] = AVG(1); x2[2] = AVG(2);
-                        sr = (PROD(2) + PROD(1)) / (SQ(xn[2] - xo[2]) + SQ(xn[1] - xo[1]));
-                        x2[0] = RBX(0);
-                        break;
-                    case 4: x2[0] = AVG(0); sr = RATIO(0); x2[1] = RBX(1); x2[2] = RBX(2); break;
-                    case 5:
-                        x2[0] = AVG(0); x2[2] = AVG(2);
-                        sr = (PROD(2) + PROD(0)) / (SQ(xn[2] - xo[2]) + SQ(xn[0] - xo[0]));
-                        x2[1] = RBX(1);
-                        break;
-                    case 6:
-                        x2[0] = AVG(0); x2[1] = AVG(1);
-                        sr = (PROD(1) + PROD(0)) / (SQ(xn[1] - xo[1]) + SQ(xn[0] - xo[0]));
-                        x2[2] = RBX(2);
-                        break;
-                    case 7: x2[0] = AVG(0); x2[1] = AVG(1); x2[2] = AVG(2); break;
-                    default: break;
-                }
+                    switch (m) {
+                        case 1: x2[2] = AVG(2); sr = RATIO(2); x2[0] = RBX(0); x2[1] = RBX(1); break;
+                        case 2: x2[1] = AVG(1); sr = RATIO(1); x2[0] = RBX(0); x2[2] = RBX(2); break;
+                        case 3:
+                            x2[1] = AVG(1); x2[2] = AVG(2);
+                            sr = (PROD(2) + PROD(1)) / (SQ(xn[2] - xo[2]) + SQ(xn[1] - xo[1]));
+                            x2[0] = RBX(0);
+                            break;
+                        case 4: x2[0] = AVG(0); sr = RATIO(0); x2[1] = RBX(1); x2[2] = RBX(2); break;
+                        case 5:
+                            x2[0] = AVG(0); x2[2] = AVG(2);
+                            sr = (PROD(2) + PROD(0)) / (SQ(xn[2] - xo[2]) + SQ(xn[0] - xo[0]));
+                            x2[1] = RBX(1);
+                            break;
+                        case 6:
+                            x2[0] = AVG(0); x2[1] = AVG(1);
+                            sr = (PROD(1) + PROD(0)) / (SQ(xn[1] - xo[1]) + SQ(xn[0] - xo[0]));
+                            x2[2] = RBX(2);
+                            break;
+                        case 7: x2[0] = AVG(0); x2[1] = AVG(1); x2[2] = AVG(2); break;
+                        default: break;
+                    }
 #undef AVG
 #undef RATIO
 #undef PROD
 #undef RBX
 #undef SQ
-                // one segment (xo -> xn) without a crossing, else xo -> x2 -> xn;
-                // one copy of pqr in the loop body keeps the kernel's code small
-                // (the front end starved on three inlined copies)
-                const int nseg = (m >= 1 && m <= 7) ? 2 : 1;
-#pragma unroll 1
-                for (int sg = 0; sg < nseg; sg++) {
-                    int iv[3];
-                    double sa[3], sb[3];
+                    // the first segment here: xo -> xn, or xo -> x2 when the step
+                    // crosses a cell-centre plane.  The second, x2 -> xn, goes to
+                    // the warp's queue and is deposited with the warp's other
+                    // crossings, 16 to 32 at a time, so that a few crossing lanes do
+                    // not make the whole warp run the deposit twice.
+                    const bool cross = m >= 1 && m <= 7;
+                    double sb[3];
 #pragma unroll
-                    for (int d = 0; d < 3; d++) {
-                        iv[d] = sg ? i2[d] : i1[d];
-                        sa[d] = sg ? x2[d] : xo[d];
-                        sb[d] = (nseg == 2 && sg == 0) ? x2[d] : xn[d];
-                    }
-                    pqr_plain<LO32>(sJ, inv_q, lo_scale, nn, SY, SZ, bi, bl, bk, iv, sa, sb, mw, hx, hy, hz, rc, x0,
-                                    y0, z0, bad);
-                }
-            }
-            x = reflect_plain(xn[0], g.lx);
-            y = reflect_plain(xn[1], g.ly);
-            z = reflect_plain(xn[2], g.lz);
-
-            // ---- flyDirection (cell.h:694-701) and the receivers of K8
-            int dxd = (((x > x0 + hx) && (x < x0 + 2 * hx)) || ((x < hx) && (i == g.nx - 1)))
-                          ? 2 : (((x < x0) || ((x > g.lx - hx) && (i == 0))) ? 0 : 1);
-            int dyd = (((y > y0 + hy) && (y < y0 + 2 * hy)) || ((y < hy) && (l == g.ny - 1)))
-                          ? 2 : (((y < y0) || ((y > g.ly - hy) && (l == 0))) ? 0 : 1);
-            int dzd = (((z > z0 + hz) && (z < z0 + 2 * hz)) || ((z < hz) && (k == g.nz - 1)))
-                          ? 2 : (((z < z0) || ((z > g.lz - hz) && (k == 0))) ? 0 : 1);
-            int newcell = cell;
-            bool leave = false;
-            int rx[3], ry[3], rz[3], nrx = 1, nry = 1, nrz = 1;
-            if (dxd * 9 + dyd * 3 + dzd != 13) {
-                nrx = receivers(x, i, g.nx, hx, rx);
-                nry = receivers(y, l, g.ny, hy, ry);
-                nrz = receivers(z, k, g.nz, hz, rz);
-                int ncopy = nrx * nry * nrz;
-                if (ncopy == 1 && g.tile_of_cell(rx[0], ry[0], rz[0]) == t) {
-                    newcell = g.cell_of(rx[0], ry[0], rz[0]);
-                } else {
-                    leave = true;
-                    if (ncopy == 0) dropped++;
-                    if (ncopy > 1) dup++;
-                    if (ncopy > 0) {
-                        unsigned e = atomicAdd(&P.st->out_count, (unsigned)ncopy);
-                        if (e + ncopy > P.out_cap) {
-                            bad |= ST_OUTBOX;
+                    for (int d = 0; d < 3; d++) sb[d] = cross ? x2[d] : xn[d];
+                    pqr_plain<LO32>(sJ, inv_q, lo_scale, nn, SY, SZ, bi, bl, bk, i1, xo, sb, mw, hx, hy, hz, rc, x0, y0,
+                                    z0, bad);
+                    if (cross) {
+                        if (i2[0] >= 2 && i2[0] <= 3 && i2[1] >= 2 && i2[1] <= 3 && i2[2] >= 2 && i2[2] <= 3) {
+                            const int e = atomicAdd(&sQn[warp], 1);  // < 15 + 32: drained at 16
+#pragma unroll
+                            for (int d = 0; d < 3; d++) {
+                                qd[d * kQPlain + e] = x2[d];
+                                qd[(3 + d) * kQPlain + e] = xn[d];
+                            }
+                            qc[e] = ((((bi + 2) * g.ty + (bl + 2)) * g.tz + (bk + 2)) << 3) | (i2[0] - 2) |
+                                    ((i2[1] - 2) << 1) | ((i2[2] - 2) << 2);
                         } else {
-                            for (int a = 0; a < nrx; a++)
-                                for (int b = 0; b < nry; b++)
-                                    for (int c = 0; c < nrz; c++) {
-                                        OutPlain o;
-                                        o.x = x; o.y = y; o.z = z; o.px = pu; o.py = pv; o.pz = pw;
-                                        o.cell = g.cell_of(rx[a], ry[b], rz[c]);
-                                        o.species = s;
-                                        outbox[e++] = o;
-                                    }
-                            moved++;
+                            bad |= ST_STENCIL;  // pqr's own stencil check
                         }
                     }
                 }
+                x = reflect_plain(xn[0], g.lx);
+                y = reflect_plain(xn[1], g.ly);
+                z = reflect_plain(xn[2], g.lz);
+
+                // ---- flyDirection (cell.h:694-701) and the receivers of K8
+                int dxd = (((x > x0 + hx) && (x < x0 + 2 * hx)) || ((x < hx) && (i == g.nx - 1)))
+                              ? 2 : (((x < x0) || ((x > g.lx - hx) && (i == 0))) ? 0 : 1);
+                int dyd = (((y > y0 + hy) && (y < y0 + 2 * hy)) || ((y < hy) && (l == g.ny - 1)))
+                              ? 2 : (((y < y0) || ((y > g.ly - hy) && (l == 0))) ? 0 : 1);
+                int dzd = (((z > z0 + hz) && (z < z0 + 2 * hz)) || ((z < hz) && (k == g.nz - 1)))
+                              ? 2 : (((z < z0) || ((z > g.lz - hz) && (k == 0))) ? 0 : 1);
+                int newcell = cell;
+                bool leave = false;
+                int rx[3], ry[3], rz[3], nrx = 1, nry = 1, nrz = 1;
+                if (dxd * 9 + dyd * 3 + dzd != 13) {
+                    nrx = receivers(x, i, g.nx, hx, rx);
+                    nry = receivers(y, l, g.ny, hy, ry);
+                    nrz = receivers(z, k, g.nz, hz, rz);
+                    int ncopy = nrx * nry * nrz;
+                    if (ncopy == 1 && g.tile_of_cell(rx[0], ry[0], rz[0]) == t) {
+                        newcell = g.cell_of(rx[0], ry[0], rz[0]);
+                    } else {
+                        leave = true;
+                        if (ncopy == 0) dropped++;
+                        if (ncopy > 1) dup++;
+                        if (ncopy > 0) {
+                            unsigned e = atomicAdd(&P.st->out_count, (unsigned)ncopy);
+                            if (e + ncopy > P.out_cap) {
+                                bad |= ST_OUTBOX;
+                            } else {
+                                for (int a = 0; a < nrx; a++)
+                                    for (int b = 0; b < nry; b++)
+                                        for (int c = 0; c < nrz; c++) {
+                                            OutPlain o;
+                                            o.x = x; o.y = y; o.z = z; o.px = pu; o.py = pv; o.pz = pw;
+                                            o.cell = g.cell_of(rx[a], ry[b], rz[c]);
+                                            o.species = s;
+                                            outbox[e++] = o;
+                                        }
+                                moved++;
+                            }
+                        }
+                    }
+                }
+                if (leave) {
+                    S.cell[slot] = -1;
+                    int hpos = atomicAdd(&sNHoles, 1);
+                    if (hpos < kHoleMax) sHoles[hpos] = j;
+                    else bad |= ST_HOLES;
+                } else {
+                    S.cell[slot] = newcell;
+                    S.x[slot] = x; S.y[slot] = y; S.z[slot] = z;
+                    S.px[slot] = pu; S.py[slot] = pv; S.pz[slot] = pw;
+                }
+            }  // particle
+            // ---- the warp's queued second segments, one per lane
+            __syncwarp();
+            qn = sQn[warp];
+            if (qn >= (tail ? 1 : 16)) {
+                const int d = qn < 32 ? qn : 32;
+                if (lane < d) {
+                    const int e = qn - d + lane;
+                    const int code = qc[e], lc = code >> 3;
+                    const int a = lc / (g.ty * g.tz), b = (lc / g.tz) % g.ty, c = lc % g.tz;
+                    const int qi = i0 + a, ql = l0 + b, qk = k0 + c;
+                    const int iv[3] = {2 + (code & 1), 2 + ((code >> 1) & 1), 2 + ((code >> 2) & 1)};
+                    double sa[3], sb[3];
+#pragma unroll
+                    for (int dd = 0; dd < 3; dd++) {
+                        sa[dd] = qd[dd * kQPlain + e];
+                        sb[dd] = qd[(3 + dd) * kQPlain + e];
+                    }
+                    pqr_plain<LO32>(sJ, inv_q, lo_scale, nn, SY, SZ, a - 2, b - 2, c - 2, iv, sa, sb, mw, hx, hy, hz,
+                                    rc, (double)qi * hx, (double)ql * hy, (double)qk * hz, bad);
+                }
+                qn -= d;
+                __syncwarp();
+                if (lane == 0) sQn[warp] = qn;
             }
-            if (leave) {
-                S.cell[slot] = -1;
-                int hpos = atomicAdd(&sNHoles, 1);
-                if (hpos < kHoleMax) sHoles[hpos] = j;
-                else bad |= ST_HOLES;
-            } else {
-                S.cell[slot] = newcell;
-                S.x[slot] = x; S.y[slot] = y; S.z[slot] = z;
-                S.px[slot] = pu; S.py[slot] = pv; S.pz[slot] = pw;
-            }
+            __syncwarp();
         }
         __syncthreads();
         // ---- compaction of the tile bin (replaces GPU_MakeDepartureLists_rm, kernels.cu:219-242)
@@ -633,7 +683,8 @@ void e_ghosts_mixed(const Grid &g, float *Ex, float *Ey, float *Ez, int periodic
 
 size_t push_smem_plain(const Grid &g) {
     size_t nn = (size_t)(g.tx + 2) * (g.ty + 2) * (g.tz + 2);
-    return 6 * nn * sizeof(double) + 6 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int);
+    return 6 * nn * sizeof(double) + 6 * nn * sizeof(unsigned long long) + 2 * kHoleMax * sizeof(int) +
+           (size_t)(kPlainThreads / 32) * kQPlain * (6 * sizeof(double) + sizeof(int));
 }
 
 cudaError_t launch_push_plain(const StepParams &p, bool lo32, cudaStream_t s) {
