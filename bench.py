@@ -710,6 +710,15 @@ def species_of(cfg):
     return configs.species_table(cfg["ppc"], sp), sp
 
 
+NONUNIFORM_NOTE = ("the CPU path's generator (the oracle's restatement of the seeded device generator) covers the "
+                   "uniform configurations c0-c3; this configuration's density profile is generated on the device "
+                   "only, so the CPU figures are the uniform configurations' (cpu_baseline.configs)")
+
+
+def uniform(cfg) -> bool:
+    return not any("profile" in s for s in species_of(cfg)[1])
+
+
 def cpu_sim(cfg, cells, threads, kind):
     """A CPU simulation of `cells` at the configuration's density: the
     reference's own functions (kind "reference", oracle/_ref) or the C
@@ -767,9 +776,12 @@ def cpu_baseline(args, cfg):
     configs = importlib.import_module("0buf_b200.configs")
     thr = cpu_threads()
     kind = ref_kind()
-    head = cpu_time(cfg, REF_SAMPLE_CELLS, thr, kind, args.cpu_seconds)
-    head["sample"] += (f" -- a periodic sub-box of the {'x'.join(map(str, cfg['cells']))}-cell workload at its "
-                       f"density; {'reference functions compiled for the host (oracle/_ref)' if kind == 'reference' else 'C restatement (oracle/cpu_pic.c)'}")
+    if uniform(cfg):
+        head = cpu_time(cfg, REF_SAMPLE_CELLS, thr, kind, args.cpu_seconds)
+        head["sample"] += (f" -- a periodic sub-box of the {'x'.join(map(str, cfg['cells']))}-cell workload at its "
+                           f"density; {'reference functions compiled for the host (oracle/_ref)' if kind == 'reference' else 'C restatement (oracle/cpu_pic.c)'}")
+    else:
+        head = {"value": None, "unit": UNIT, "note": NONUNIFORM_NOTE}
     out = dict(head)
     out["configs"] = {}
     runs = [("c0", "reference" if kind == "reference" else "port", thr, 4.0, True),
@@ -794,6 +806,8 @@ def run_reference(args):
     on all host cores."""
     configs = importlib.import_module("0buf_b200.configs")
     cfg = workload_cfg(args, configs)
+    if not uniform(cfg):
+        return {"impl": "reference", "unavailable": NONUNIFORM_NOTE}
     threads = cpu_threads()
     kind = ref_kind()
     sim = cpu_sim(cfg, REF_SAMPLE_CELLS, threads, kind)
