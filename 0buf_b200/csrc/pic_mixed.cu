@@ -523,7 +523,7 @@ __global__ void PIC_MIXED_BOUNDS k_push_mixed(const __grid_constant__ MixedMaps 
             for (int idx = lane; idx < 3 * nn; idx += 32) {
                 if (myJ[idx]) {
                     const int w = atomicExch(&myJ[idx], 0);
-                    if (w) atomicAdd(&sJ[idx], (unsigned long long)rescale(w, sh));
+                    if (w) shared_add64(&sJ[idx], rescale(w, sh));
                 }
             }
             __syncwarp();
