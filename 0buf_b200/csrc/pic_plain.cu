@@ -231,14 +231,14 @@ __device__ __forceinline__ int receivers(double x, int c, int N, double h, int o
     return n;
 }
 
-// 512 threads, two CTAs per SM: 32 warps per SM at 64 registers (ptxas
-// spills ~300 bytes).  The kernel waits on shared-atomic round trips and FP64
-// dependency chains, and the extra warps hide them: c2 push 208.7 ms against
-// 246.5 ms with 256 threads at 126 registers (320: 229.8, 384: 219.8,
-// 448: 214.5, 256 x 3 CTAs: 218.4); with one pqr call site, 163.3 ms against
-// 189.4 at 384 threads
+// 256 threads, two CTAs per SM: 16 warps per SM at up to 126 registers, no
+// spills.  While 64-bit shared atomics were compare-and-swap loops, 512-thread
+// CTAs at 64 registers (32 warps, ~240 B of spills) hid their round trips
+// better (c2 push 208.7 ms against 246.5 at 256 threads); with the split
+// 64-bit add (shared_add64) the atomics cost nothing measurable and 256
+// threads win: 71.1 ms against 72.7 (384: 75.0, 448: 76.0).
 #ifndef PIC_PLAIN_THREADS
-#define PIC_PLAIN_THREADS 512
+#define PIC_PLAIN_THREADS 256
 #endif
 #ifndef PIC_PLAIN_MIN_BLOCKS
 #define PIC_PLAIN_MIN_BLOCKS 2
