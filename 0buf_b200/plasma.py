@@ -248,12 +248,6 @@ class PicSimulation:
         self.lib.pic_step_counters(self.h, c.ctypes.data_as(_capi.I64))
         return c
 
-    def sort_stats(self) -> np.ndarray:
-        """[depositing particles outside their warp's cell groups, bin sorts run] of the last step."""
-        c = np.zeros(2, np.int64)
-        self.lib.pic_sort_stats(self.h, c.ctypes.data_as(_capi.I64))
-        return c
-
     def timings(self) -> np.ndarray:
         """[b_half, push kernel, migration arrivals, second field half, whole step] in ms."""
         t = np.zeros(5, np.float32)
