@@ -82,7 +82,7 @@ typedef struct pic_config {
     pic_species species[PIC_MAX_SPECIES];
     double capacity_slack;   /* particle slots per tile = count * (1 + slack) + pad; 0 -> 0.25 */
     double outbox_fraction;  /* outbox slots = fraction * total capacity + 65536; 0 -> 0.04 */
-    int tile[3];             /* cells per tile (x, y, z); 0 -> automatic: 4 x 4 x 16 (FP64 form),
+    int tile[3];             /* cells per tile (x, y, z); 0 -> automatic: 8 x 4 x 8 (FP64 form),
                                 4 x 4 x 12 (FP32 form), capped by the grid. tile[2] % 4 == 0 */
     int capacity_pad;        /* extra slots per tile; negative -> 64 */
     int reserved[7];
@@ -271,9 +271,11 @@ typedef struct pic_grads {
     double *d_p0;       /* in: host array of 3*n doubles (px, py, pz of each particle) or NULL;
                            particles in the order pic_get_particles gave at the
                            start of the forward -- this handle's bin order, which
-                           depends on its tiling (the FP32 form tiles z by 12,
-                           the FP64 form by 16), so match particles by their
-                           state, not by index, across handles */
+                           depends on its tiling (FP64 form 8x4x8 cells, FP32
+                           form 4x4x12), so match particles by their state, not
+                           by index, across handles; bins keep the load (or
+                           generation) order inside a cell, so a stable sort by
+                           cell gives an order common to all tilings */
     double reserved[4];
 } pic_grads;
 

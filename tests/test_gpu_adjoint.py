@@ -144,18 +144,23 @@ def test_mixed_forward_is_the_step(pkg):
 def test_mixed_gradient_matches_fp64(pkg):
     """The FP32 adjoint (FP32 per particle, FP64 field adjoints) against the
     FP64 adjoint and FP64 central differences of the same loss."""
-    grads = {}
+    grads, order = {}, {}
     for prec in ("fp64", "fp32"):
         with make(pkg, precision=prec) as sim:
+            p = sim.particles(BEAM)
             if prec == "fp64":
-                base = sim.particles(BEAM)
+                base = p
+            # d_p0 rows follow the handle's bin order, which depends on its
+            # tiling; the bins keep the generation order inside a cell, so a
+            # stable sort by cell gives one order for both forms
+            order[prec] = np.argsort(p["cell"], kind="stable")
             sim.forward(STEPS, 7)
             grads[prec] = sim.backward(**LOSS)
     g64, g32 = grads["fp64"], grads["fp32"]
     assert abs(g32["loss"] - g64["loss"]) / g64["loss"] < 1e-4
     assert abs(g32["d_drift"][0] - g64["d_drift"][0]) / abs(g64["d_drift"][0]) < 1e-3
     assert abs(g32["d_vth"] - g64["d_vth"]) / abs(g64["d_vth"]) < 1e-3
-    assert rel_l2(g32["d_p0"], g64["d_p0"]) < 1e-2
+    assert rel_l2(g32["d_p0"][order["fp32"]], g64["d_p0"][order["fp64"]]) < 1e-2
     n = base["x"].size
     e_x = np.zeros((n, 3))
     e_x[:, 0] = 1.0
