@@ -405,7 +405,7 @@ int do_e_ghosts(pic_handle *h) {
     else
         e_ghosts_mixed(h->g, (float *)h->f[PIC_EX], (float *)h->f[PIC_EY], (float *)h->f[PIC_EZ], per, h->stream);
     CK(cudaGetLastError(), "e_ghosts");
-    h->launches += 2;
+    h->launches += 1;
     return PIC_OK;
 }
 

@@ -19,6 +19,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <utility>
 #include "pic0buf.h"
 
 namespace pic {
@@ -76,6 +77,35 @@ struct Grid {
         return ((i / tx) * nty + (l / ty)) * ntz + (k / tz);
     }
 };
+
+// The field kernels after the push (J fold, B, E, E ghosts) run as a chain
+// of programmatically dependent launches: each is launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, and every CTA first
+// waits in hardware for the previous grid to complete and flush
+// (griddepcontrol.wait), then lets the next grid be scheduled
+// (griddepcontrol.launch_dependents).  The next grid's CTAs thus take SM
+// slots as this grid's retire and start the moment it is done, instead of
+// after a full launch gap; every CTA of a grid has started before the next
+// grid's are scheduled, so waiting CTAs never hold slots the running grid
+// needs.  For a kernel launched without the attribute both are no-ops.
+__device__ __forceinline__ void chain_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... P, typename... A>
+inline cudaError_t launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, cudaStream_t s, A &&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 // Tile current accumulation in 64-bit fixed point.  Each contribution is
 // rounded to the tile's quantum q = 2^(E-62), where 2^E exceeds

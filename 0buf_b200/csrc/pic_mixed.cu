@@ -51,6 +51,7 @@ template <bool TWICE>
 __global__ void k_b_half_mixed(Grid g, const float *__restrict__ Ex, const float *__restrict__ Ey,
                                const float *__restrict__ Ez, float *Hx, float *Hy, float *Hz, float cx, float cy,
                                float cz) {
+    chain_enter();
     const int nq = g.pz / 4;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.NY * nq) return;
@@ -91,6 +92,7 @@ __global__ void k_e_update_mixed(Grid g, float *Ex, float *Ey, float *Ez, const 
                                  const float *__restrict__ Hy, const float *__restrict__ Hz,
                                  const double *__restrict__ Jx, const double *__restrict__ Jy,
                                  const double *__restrict__ Jz, float cx, float cy, float cz, double tau) {
+    chain_enter();
     const int nq = g.pz / 4;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.NY * nq) return;
@@ -881,18 +883,20 @@ static inline dim3 plane_grid(const Grid &g) {
 
 void yee_b_half_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s) {
     float cx = (float)(g.tau / g.hx), cy = (float)(g.tau / g.hy), cz = (float)(g.tau / g.hz);
-    k_b_half_mixed<false><<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], cx, cy, cz);
+    launch_chained(k_b_half_mixed<false>, plane_grid(g), dim3(kPlaneThreads), s, g, E[0], E[1], E[2], H[0], H[1], H[2],
+                   cx, cy, cz);
 }
 
 void yee_b_both_mixed(const Grid &g, float *const E[3], float *const H[3], cudaStream_t s) {
     float cx = (float)(g.tau / g.hx), cy = (float)(g.tau / g.hy), cz = (float)(g.tau / g.hz);
-    k_b_half_mixed<true><<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], cx, cy, cz);
+    launch_chained(k_b_half_mixed<true>, plane_grid(g), dim3(kPlaneThreads), s, g, E[0], E[1], E[2], H[0], H[1], H[2],
+                   cx, cy, cz);
 }
 
 void yee_e_update_mixed(const Grid &g, float *const E[3], float *const H[3], double *const J[3], cudaStream_t s) {
     float cx = (float)(g.tau / g.hx), cy = (float)(g.tau / g.hy), cz = (float)(g.tau / g.hz);
-    k_e_update_mixed<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, E[0], E[1], E[2], H[0], H[1], H[2], J[0], J[1], J[2], cx,
-                                                     cy, cz, g.tau);
+    launch_chained(k_e_update_mixed, plane_grid(g), dim3(kPlaneThreads), s, g, E[0], E[1], E[2], H[0], H[1], H[2], J[0],
+                   J[1], J[2], cx, cy, cz, g.tau);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link

@@ -22,6 +22,7 @@ namespace {
 __global__ void k_b_half_plain(Grid g, const double *__restrict__ Ex, const double *__restrict__ Ey,
                                const double *__restrict__ Ez, double *Hx, double *Hy, double *Hz, double *Qx,
                                double *Qy, double *Qz, double cx, double cy, double cz) {
+    chain_enter();
     // one thread per node of an x plane (l, k flattened: no idle z tail)
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.NY * g.NZ) return;
@@ -51,6 +52,7 @@ __global__ void k_b_half_plain(Grid g, const double *__restrict__ Ex, const doub
 // emh2_Element (kernels.cu:1024-1049) over the same ranges
 __global__ void k_b_complete_plain(Grid g, double *Hx, double *Hy, double *Hz, const double *__restrict__ Qx,
                                    const double *__restrict__ Qy, const double *__restrict__ Qz) {
+    chain_enter();
     // one thread per node of an x plane (l, k flattened: no idle z tail)
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.NY * g.NZ) return;
@@ -70,6 +72,7 @@ __global__ void k_e_update_plain(Grid g, double *Ex, double *Ey, double *Ez, con
                                  const double *__restrict__ Hy, const double *__restrict__ Hz,
                                  const double *__restrict__ Jx, const double *__restrict__ Jy,
                                  const double *__restrict__ Jz, double cx, double cy, double cz, double tau) {
+    chain_enter();
     // one thread per node of an x plane (l, k flattened: no idle z tail)
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.NY * g.NZ) return;
@@ -103,6 +106,7 @@ __device__ __forceinline__ Line line_of(const Grid &g, int dir, int a, int b) {
 // three components; SetPeriodicCurrents order (gpu_plasma.h:926-993) is per
 // component x, y, z, and the components are independent arrays.
 __global__ void k_j_fold(Grid g, double *Jx, double *Jy, double *Jz, int dir) {
+    chain_enter();
     int A = dir == 0 ? g.NY : g.NX;
     int B = dir == 2 ? g.NY : g.NZ;
     int N = dir == 0 ? g.NX : (dir == 1 ? g.NY : g.NZ);  // Naxis + 2
@@ -128,22 +132,56 @@ struct GhostPass {
     void *E;
     int dir, s1, e1, s2, e2, N;
 };
+// The reference runs the passes in two rounds, A then B.  No node is written
+// by both rounds, and no A pass reads a node that B writes; the only order
+// between them is B reading ghosts that A wrote.  All passes are copies, so B
+// reading A's source node instead gives the same bits, and both rounds run
+// in one launch: passes p[0 .. nA) are A, p[nA .. n) are B.
 struct GhostPasses {
-    GhostPass p[3];
-    int n;
+    GhostPass p[6];
+    int nA, n;
 };
+// node (c[0], c[1], c[2]) of array E, moved to the node an A pass copies into
+// it when an A pass writes it
+__device__ __forceinline__ size_t ghost_source(const Grid &g, const GhostPasses &P, const void *E, int c[3]) {
+    for (int a = 0; a < P.nA; a++) {
+        const GhostPass &q = P.p[a];
+        if (q.E != E) continue;
+        const int d = q.dir;
+        const int ca = d == 0 ? c[1] : c[0], cb = d == 2 ? c[1] : c[2];  // the line's (a, b), as in line_of
+        if (ca < q.s1 || ca > q.e1 || cb < q.s2 || cb > q.e2) continue;
+        if (c[d] == 0) c[d] = q.N;
+        else if (c[d] == q.N + 1) c[d] = 1;
+    }
+    return g.node(c[0], c[1], c[2]);
+}
 template <typename T>
 __global__ void k_e_ghosts(Grid g, GhostPasses P) {
+    chain_enter();
     if ((int)blockIdx.y >= P.n) return;
-    GhostPass q = P.p[blockIdx.y];
-    int A = q.e1 - q.s1 + 1, B = q.e2 - q.s2 + 1;
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const GhostPass q = P.p[blockIdx.y];
+    const int A = q.e1 - q.s1 + 1, B = q.e2 - q.s2 + 1;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= A * B) return;
-    Line L = line_of(g, q.dir, q.s1 + idx / B, q.s2 + idx % B);
-    T *E = (T *)q.E + L.base;
-    E[0] = E[(size_t)q.N * L.stride];
-    E[(size_t)(q.N + 1) * L.stride] = E[L.stride];
+    const int la = q.s1 + idx / B, lb = q.s2 + idx % B;
+    const Line L = line_of(g, q.dir, la, lb);
+    T *E = (T *)q.E;
+    size_t srcN = L.base + (size_t)q.N * L.stride, src1 = L.base + L.stride;
+    if ((int)blockIdx.y >= P.nA) {
+        // line coordinates (x along dir) as in line_of
+        int cN[3], c1[3];
+        const int d = q.dir, o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+        cN[o1] = c1[o1] = la;
+        cN[o2] = c1[o2] = lb;
+        cN[d] = q.N;
+        c1[d] = 1;
+        srcN = ghost_source(g, P, q.E, cN);
+        src1 = ghost_source(g, P, q.E, c1);
+    }
+    E[L.base] = E[srcN];
+    E[L.base + (size_t)(q.N + 1) * L.stride] = E[src1];
 }
+
 
 // ------------------------------------------------------- particle push --
 enum : int { kCE = 5 };  // CellExtent, cell.h:23
@@ -624,20 +662,19 @@ static inline dim3 plane_grid(const Grid &g) {
 void yee_b_half_plain(const Grid &g, double *const F[12], cudaStream_t s) {
     // getMagneticFieldTimeMeshFactors, gpu_plasma.h:512-522
     double cx = g.tau / (g.hx), cy = g.tau / (g.hy), cz = g.tau / g.hz;
-    k_b_half_plain<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, F[PIC_EX], F[PIC_EY], F[PIC_EZ], F[PIC_HX], F[PIC_HY],
-                                                   F[PIC_HZ], F[PIC_QX], F[PIC_QY], F[PIC_QZ], cx, cy, cz);
+    launch_chained(k_b_half_plain, plane_grid(g), dim3(kPlaneThreads), s, g, F[PIC_EX], F[PIC_EY], F[PIC_EZ], F[PIC_HX],
+                   F[PIC_HY], F[PIC_HZ], F[PIC_QX], F[PIC_QY], F[PIC_QZ], cx, cy, cz);
 }
 
 void yee_b_complete_plain(const Grid &g, double *const F[12], cudaStream_t s) {
-    k_b_complete_plain<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, F[PIC_HX], F[PIC_HY], F[PIC_HZ], F[PIC_QX],
-                                                       F[PIC_QY], F[PIC_QZ]);
+    launch_chained(k_b_complete_plain, plane_grid(g), dim3(kPlaneThreads), s, g, F[PIC_HX], F[PIC_HY], F[PIC_HZ],
+                   F[PIC_QX], F[PIC_QY], F[PIC_QZ]);
 }
 
 void yee_e_update_plain(const Grid &g, double *const F[12], cudaStream_t s) {
     double cx = g.tau / (g.hx), cy = g.tau / (g.hy), cz = g.tau / g.hz;
-    k_e_update_plain<<<plane_grid(g), kPlaneThreads, 0, s>>>(g, F[PIC_EX], F[PIC_EY], F[PIC_EZ], F[PIC_HX],
-                                                     F[PIC_HY], F[PIC_HZ], F[PIC_JX], F[PIC_JY], F[PIC_JZ],
-                                                     cx, cy, cz, g.tau);
+    launch_chained(k_e_update_plain, plane_grid(g), dim3(kPlaneThreads), s, g, F[PIC_EX], F[PIC_EY], F[PIC_EZ],
+                   F[PIC_HX], F[PIC_HY], F[PIC_HZ], F[PIC_JX], F[PIC_JY], F[PIC_JZ], cx, cy, cz, g.tau);
 }
 
 
@@ -646,33 +683,34 @@ void j_fold(const Grid &g, double *Jx, double *Jy, double *Jz, cudaStream_t s) {
         int A = dir == 0 ? g.NY : g.NX;
         int B = dir == 2 ? g.NY : g.NZ;
         int n = A * B;
-        k_j_fold<<<(n + 127) / 128, 128, 0, s>>>(g, Jx, Jy, Jz, dir);
+        launch_chained(k_j_fold, dim3((n + 127) / 128), dim3(128), s, g, Jx, Jy, Jz, dir);
     }
 }
 
 // ElectricFieldComponentEvaluatePeriodic for Ex, Ey, Ez (gpu_plasma.h:432-452,
 // arguments gpu_plasma.h:486-505).  Reference mode skips the y pass of Ex and
-// Ez; periodic mode performs it.  Launch A holds the first pass of each
-// component, launch B the second (Ey's z pass reads the x ghosts of A).
+// Ez; periodic mode performs it.  Round A holds the first pass of each
+// component, round B the second; both run in one launch (GhostPasses).
 template <typename T>
 static void e_ghosts_t(const Grid &g, T *Ex, T *Ey, T *Ez, int periodic, cudaStream_t s) {
     int Nx = g.nx, Ny = g.ny, Nz = g.nz;
-    GhostPasses A{}, B{};
+    GhostPasses P{};
     int maxn = 0;
-    auto add = [&](GhostPasses &P, T *E, int dir, int s1, int e1, int s2, int e2, int N) {
+    auto add = [&](T *E, int dir, int s1, int e1, int s2, int e2, int N) {
         P.p[P.n++] = GhostPass{(void *)E, dir, s1, e1, s2, e2, N};
         int n = (e1 - s1 + 1) * (e2 - s2 + 1);
         if (n > maxn) maxn = n;
     };
-    if (periodic) add(A, Ex, 1, 0, Nx, 1, Nz, Ny);
-    add(A, Ey, 0, 0, Ny, 1, Nz, Nx);
-    add(A, Ez, 0, 1, Ny, 0, Nz, Nx);
-    add(B, Ex, 2, 0, Nx, 0, Ny + 1, Nz);
-    add(B, Ey, 2, 0, Nx + 1, 0, Ny, Nz);
-    if (periodic) add(B, Ez, 1, 0, Nx + 1, 0, Nz, Ny);
-    dim3 grid((maxn + 127) / 128, 3);
-    k_e_ghosts<T><<<grid, 128, 0, s>>>(g, A);
-    k_e_ghosts<T><<<grid, 128, 0, s>>>(g, B);
+    // round A: the first pass of each component
+    if (periodic) add(Ex, 1, 0, Nx, 1, Nz, Ny);
+    add(Ey, 0, 0, Ny, 1, Nz, Nx);
+    add(Ez, 0, 1, Ny, 0, Nz, Nx);
+    P.nA = P.n;
+    // round B: the second (Ey's z pass reads the x ghosts of round A)
+    add(Ex, 2, 0, Nx, 0, Ny + 1, Nz);
+    add(Ey, 2, 0, Nx + 1, 0, Ny, Nz);
+    if (periodic) add(Ez, 1, 0, Nx + 1, 0, Nz, Ny);
+    launch_chained(k_e_ghosts<T>, dim3((maxn + 127) / 128, P.n), dim3(128), s, g, P);
 }
 void e_ghosts_plain(const Grid &g, double *Ex, double *Ey, double *Ez, int periodic, cudaStream_t s) {
     e_ghosts_t<double>(g, Ex, Ey, Ez, periodic, s);

@@ -49,8 +49,8 @@ BYTES_PER_CELL_UPDATE = {"fp32": 72, "fp64": 120}
 NCU_TRAFFIC_PER_PARTICLE = {"fp32": 2.820e9 / 50331648, "fp64": 5.271e9 / 50331648}
 KERNELS_PER_STEP_NOTE = {
     "fp32": "push (forms the B half step of its staged tile), insert, clamp, j_fold x3, b_half twice in one pass, "
-            "e_update, e_ghosts x2; plus k_contribution_bound once per species after a load",
-    "fp64": "b_half, push, insert, clamp, j_fold x3, b_complete, e_update, e_ghosts x2"}
+            "e_update, e_ghosts (both rounds in one launch); plus k_contribution_bound once per species after a load",
+    "fp64": "b_half, push, insert, clamp, j_fold x3, b_complete, e_update, e_ghosts"}
 
 
 def peaks():
