@@ -68,6 +68,11 @@ struct pic_handle {
     // (valid while tile_cap_valid; cleared whenever a species' bins change)
     int tile_cap_valid;
     int64_t tile_cap_max;
+    // staging of pic_load_particles_cells (cells, offsets, chunks), kept from
+    // one species' load to the next and released when the run's first push
+    // starts (release_load_scratch) or by pic_destroy
+    void *load_buf;
+    size_t load_bytes;
 };
 
 namespace pic_host {
@@ -101,6 +106,8 @@ struct ScratchGuard {
         for (void *p : bufs) dev_free(h, p);
     }
 };
+// frees the load staging (pic_load_particles_cells)
+void release_load_scratch(pic_handle *h);
 // kernel parameters of the current state (species views, fields, outbox, status)
 pic::StepParams make_params(pic_handle *h);
 // flat device list of one species (packed cell, FP64 global positions and
