@@ -484,9 +484,10 @@ def run_adjoint(args, pkg, dev):
         fd[form] = {"drift_rel_err": abs(g["d_drift"][0] - d_drift) / abs(d_drift),
                     "vth_rel_err": abs(g["d_vth"] - d_vth) / abs(d_vth), "particle_dirs_rel_err": []}
     rng = np.random.default_rng(16)
+    canon = np.argsort(base["cell"], kind="stable")  # a tiling-independent particle order
     for _ in range(args.adjoint_dirs):
         v = np.zeros((n, 3))
-        v[rng.integers(n)] = rng.standard_normal(3)
+        v[canon[rng.integers(n)]] = rng.standard_normal(3)
         f = loss_of(v, 1e-6)
         for form in ("fp64", "fp32"):
             ad = float(np.sum(grads[form]["d_p0"] * v))
@@ -531,8 +532,17 @@ def frozen_branch_check(pkg, cfg, dev, steps, base, grads):
     e_x = np.zeros((n, 3))
     e_x[:, 0] = 1.0
     dirs = {"vth": xi, "drift_x": e_x}
-    # 16 seeded dense directions over every beam particle (seeds 1..16)
-    dirs.update({f"dense_{k}": np.random.default_rng(k).standard_normal((n, 3)) for k in range(1, 17)})
+    # 16 seeded dense directions over every beam particle (seeds 1..16), drawn
+    # in a canonical particle order (by cell, generation order inside a cell:
+    # a stable sort of the bins) so that they do not depend on the tiling
+    canon = np.argsort(base["cell"], kind="stable")
+
+    def dense(k):
+        v = np.empty((n, 3))
+        v[canon] = np.random.default_rng(k).standard_normal((n, 3))
+        return v
+
+    dirs.update({f"dense_{k}": dense(k) for k in range(1, 17)})
     out = {"reference": "FP64 central differences, eps 1e-7, of the forward replaying a recorded FP64 run's "
                         "discrete choices (taps, zigzag split classes, wraps, cell moves)",
            "replay_at_eps0_rel_diff": float(f"{abs(loss(None, 0.0) - l_rec) / abs(l_rec):.3e}")}
