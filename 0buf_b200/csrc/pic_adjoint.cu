@@ -486,8 +486,11 @@ __device__ __forceinline__ int new_cell_plain(const Grid &g, int cell, int i, in
     return g.cell_of(rx, ry, rz);
 }
 
-// ---- flat forward step of all particles (push + deposit + cell update)
-__global__ void __launch_bounds__(kT) k_flat_push_plain(FlatParams P) {
+// ---- flat forward step of all particles (push + deposit + cell update).
+// Four CTAs per SM (64 registers, some spills): the kernel gathers its field
+// taps from global memory and waits on them; 32 warps per SM hide more of
+// that than 16 at 96 registers (c3 forward about 9 % faster)
+__global__ void __launch_bounds__(kT, 4) k_flat_push_plain(FlatParams P) {
     int64_t idx = spread_index(threadIdx.x);
     unsigned bad = 0;
     unsigned long long amb = 0;

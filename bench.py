@@ -399,9 +399,20 @@ def run_adjoint(args, pkg, dev):
     out = {"config": f"c3: {'x'.join(map(str, cfg['cells']))} cells, {cfg['ppc']} particles/cell/species x 3, "
                      f"{steps} steps, checkpoints every {K}, loss = sum over the last 50 steps of h^3 sum E_x^2, "
                      "gradient w.r.t. the beam's initial momenta, drift and thermal spread"}
+    import torch
     grads = {}
     base = None
     starts = {}
+    # pic_step at the same configuration, timed the same way (CUDA events on
+    # the library's stream): the comparison for the forward's per-step time
+    step_ms = {}
+    for form in ("fp64", "fp32"):
+        sim = make_sim(pkg, cfg, form, dev, 0)
+        for k in range(3):
+            sim.step(k + 1)
+        ms, _, _ = timed_steps(sim, 20, torch)
+        step_ms[form] = ms / 20
+        sim.close()
     for form in ("fp64", "fp32"):
         sim = make_sim(pkg, cfg, form, dev, 0)
         starts[form] = sim.particles(ADJ_LOSS["species"])
@@ -415,6 +426,8 @@ def run_adjoint(args, pkg, dev):
         out[form] = {"forward_ms": round(float(t[0]), 2), "backward_ms": round(float(t[1]), 2),
                      "backward_over_forward": round(float(t[1] / t[0]), 3),
                      "particle_steps_per_s_forward": round(sim_particles(cfg) * steps / (float(t[0]) / 1e3), 1),
+                     "step_ms": round(step_ms[form], 4),
+                     "forward_step_over_pic_step": round(float(t[0]) / steps / step_ms[form], 3),
                      "loss": g["loss"], "d_drift_x": float(g["d_drift"][0]), "d_vth": float(g["d_vth"])}
     # the FP64 gradient's own sensitivity to FP32 rounding: the FP64 adjoint
     # from the same initial state with every in-cell offset and momentum
