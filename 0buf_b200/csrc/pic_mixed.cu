@@ -943,6 +943,8 @@ size_t push_smem_mixed(const Grid &g) { return mixed_smem(g.tx, g.ty, g.tz).tota
 using PushMixedFn = void (*)(const MixedMaps, StepParams);
 // the instantiation for a grid's tile: fixed dimensions for the automatic tiles, else runtime
 static PushMixedFn push_mixed_fn(const Grid &g) {
+    if (g.tx == 6 && g.ty == 4 && g.tz == 8) return k_push_mixed<6, 4, 8>;
+    if (g.tx == 6 && g.ty == 4 && g.tz == 4) return k_push_mixed<6, 4, 4>;
     if (g.tx == 4 && g.ty == 4 && g.tz == 12) return k_push_mixed<4, 4, 12>;
     if (g.tx == 4 && g.ty == 4 && g.tz == 8) return k_push_mixed<4, 4, 8>;
     if (g.tx == 4 && g.ty == 4 && g.tz == 4) return k_push_mixed<4, 4, 4>;

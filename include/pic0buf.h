@@ -83,7 +83,7 @@ typedef struct pic_config {
     double capacity_slack;   /* particle slots per tile = count * (1 + slack) + pad; 0 -> 0.25 */
     double outbox_fraction;  /* outbox slots = fraction * total capacity + 65536; 0 -> 0.04 */
     int tile[3];             /* cells per tile (x, y, z); 0 -> automatic: 8 x 4 x 8 (FP64 form),
-                                4 x 4 x 12 (FP32 form), capped by the grid. tile[2] % 4 == 0 */
+                                6 x 4 x 8 (FP32 form), capped by the grid. tile[2] % 4 == 0 */
     int capacity_pad;        /* extra slots per tile; negative -> 64 */
     int reserved[7];
 } pic_config;
@@ -275,7 +275,7 @@ typedef struct pic_grads {
                            particles in the order pic_get_particles gave at the
                            start of the forward -- this handle's bin order, which
                            depends on its tiling (FP64 form 8x4x8 cells, FP32
-                           form 4x4x12), so match particles by their state, not
+                           form 6x4x8), so match particles by their state, not
                            by index, across handles; bins keep the load (or
                            generation) order inside a cell, so a stable sort by
                            cell gives an order common to all tilings */
