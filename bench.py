@@ -680,23 +680,31 @@ def run_e2e(args, dist, pkg, cfg, form, torch, n_local):
     dist.barrier()
     t0 = time.perf_counter()
     sim = pkg.PicSimulation(cfg["cells"], box, cfg["tau"], table, precision=form, device=dev)
+    t1 = time.perf_counter()
     h2d = 0
     for s, arrs in enumerate(host):
-        sim.load_particles_cells(s, *arrs)
+        sim.load_particles_cells(s, *arrs)  # returns after its last copy and scatter
         h2d += sum(a.numel() * a.element_size() for a in arrs)
+    t2 = time.perf_counter()
     energies = []
     for k in range(K):
         sim.step(k + 1)
-        energies.append(sim.energy())
+        energies.append(sim.energy())  # the step's result, read back to the host
+    t3 = time.perf_counter()
     sim.close()
     torch.cuda.synchronize()
-    ms = (time.perf_counter() - t0) * 1e3
+    t4 = time.perf_counter()
+    ms = (t4 - t0) * 1e3
+    phases = {"create": (t1 - t0) * 1e3, "load": (t2 - t1) * 1e3, "steps": (t3 - t2) * 1e3, "destroy": (t4 - t3) * 1e3}
     dist.barrier()
     t_max = dist.max(ms)
     n_total = dist.sum(n_local)
     return {"value": round(n_total * K / (t_max / 1e3), 1), "unit": UNIT,
             "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": 32, "steps": K,
-            "ms_total": round(t_max, 2),
+            "ms_total": round(t_max, 2), "phases_ms": {k: round(v, 1) for k, v in phases.items()},
+            "phases_note": "this rank's wall clock per phase; the first step also frees the load staging and sizes "
+                           "the outbox, and a multi-GB device allocation or free has taken the driver 0.5-0.9 s on "
+                           "some runs (in whichever phase makes it)",
             "path": "wall clock around pic_create + pic_load_particles_cells of every species from pinned host "
                     "memory + K x (pic_step + pic_energy read back to the host) + pic_destroy",
             "h2d_note": "the particles are loaded once; h2d_bytes_per_step is that load (28 B per particle) divided "
