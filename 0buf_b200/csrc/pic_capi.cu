@@ -352,9 +352,8 @@ bool plain_lo32(pic_handle *h) {
 int do_push_deposit(pic_handle *h, int b_half_in_push = 0) {
     int rc = need_particles(h);
     if (rc) return rc;
-    // loading is over: its staging goes, and the outbox is sized once for all
-    // species (the loads leave that to the first push)
-    release_load_scratch(h);
+    // the outbox is sized once for all species (the loads leave that to the
+    // first push)
     if ((rc = ensure_outbox(h))) return rc;
     size_t nodes = h->g.nodes_pitched();
     for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(h->f[PIC_JX + c], 0, nodes * sizeof(double), h->stream), "zero J");

@@ -69,8 +69,8 @@ struct pic_handle {
     int tile_cap_valid;
     int64_t tile_cap_max;
     // staging of pic_load_particles_cells (cells, offsets, chunks), kept from
-    // one species' load to the next and released when the run's first push
-    // starts (release_load_scratch) or by pic_destroy
+    // one species' load to the next and released by pic_destroy
+    // (release_load_scratch)
     void *load_buf;
     size_t load_bytes;
 };

@@ -115,8 +115,7 @@ int pic_load_particles_device(pic_handle *h, int species, int64_t n, const doubl
  * FP64 positions as (i + offset) * h.  Entries with a ghost/out-of-range cell
  * or an offset outside [0,1) are dropped.  Its device staging (about 16 bytes
  * per particle of the largest species loaded, plus 0.5 GB of chunks) stays
- * with the handle for the next load and is freed when the first push starts
- * (pic_step / pic_push_deposit) or by pic_destroy. */
+ * with the handle for the next load and is freed by pic_destroy. */
 int pic_load_particles_cells(pic_handle *h, int species, int64_t n, const int32_t *cell, const float *ox,
                              const float *oy, const float *oz, const float *px, const float *py, const float *pz,
                              int64_t *inserted);
