@@ -44,9 +44,9 @@ BYTES_PER_CELL_UPDATE = {"fp32": 72, "fp64": 120}
 # DRAM bytes per particle of the push kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture of 50,331,648 particles, scaled to
 # a launch by particle count since the kernel's traffic is proportional to it):
-# profiles/push_mixed_128x64x64_ncu.md (2.820 GB) and
-# profiles/push_plain_128x64x64_ncu.md (5.271 GB)
-NCU_TRAFFIC_PER_PARTICLE = {"fp32": 2.820e9 / 50331648, "fp64": 5.271e9 / 50331648}
+# profiles/push_mixed_128x64x64_ncu.md (2.830 GB) and
+# profiles/push_plain_128x64x64_ncu.md (5.267 GB)
+NCU_TRAFFIC_PER_PARTICLE = {"fp32": 2.830e9 / 50331648, "fp64": 5.267e9 / 50331648}
 KERNELS_PER_STEP_NOTE = {
     "fp32": "push (forms the B half step of its staged tile), insert, clamp, j_fold x3, b_half twice in one pass, "
             "e_update, e_ghosts (both rounds in one launch); plus k_contribution_bound once per species after a load",
