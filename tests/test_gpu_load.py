@@ -2,8 +2,9 @@
 in chunks of 2^24 particles on a second stream and binned with warp-aggregated
 per-tile counters.  A species of 2.5 chunks exported, reloaded and exported
 again gives back the same particles, entries with an invalid cell or offset
-are dropped (one of them on a chunk boundary), and an empty load leaves an
-empty species."""
+are dropped (one of them on a chunk boundary), an empty load leaves an
+empty species, and the staging that the handle keeps between loads serves
+loads of different sizes."""
 import numpy as np
 import pytest
 
@@ -64,3 +65,24 @@ def test_empty_load(pkg):
         sim.init_species(1, 4, (0.0, 0.0, 0.0), 0.01, seed=1)
         sim.step(1)
         assert sim.num_particles(0) == 0 and sim.num_particles(1) == 8 * 8 * 8 * 4
+
+
+def test_staging_reused_across_loads_of_different_sizes(pkg):
+    """The load staging stays with the handle from one load to the next and
+    grows when a larger species comes: small, larger (over one chunk), small
+    again, and a reload after a step, each exported back unchanged."""
+    cells = (160, 64, 64)
+    with make(pkg, cells) as a, make(pkg, cells) as b:
+        for s, ppc in ((0, 2), (1, 32), (2, 4)):
+            a.init_species(s, ppc, (0.0, 0.0, 0.0), 0.02, seed=7 + s)
+        src = [export(a, s) for s in range(3)]
+        assert src[0][0].size < CHUNK < src[1][0].size
+        for s in range(3):
+            assert b.load_particles_cells(s, *src[s]) == src[s][0].size
+        for s in range(3):
+            assert np.array_equal(row_keys(export(b, s)), row_keys(src[s]))
+        b.step(1)
+        assert b.load_particles_cells(0, *src[0]) == src[0][0].size
+        assert np.array_equal(row_keys(export(b, 0)), row_keys(src[0]))
+        b.step(2)
+        assert b.num_particles() == sum(x[0].size for x in src)
