@@ -387,21 +387,25 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
                 double x = S.x[slot], y = S.y[slot], z = S.z[slot];
                 double pu = S.px[slot], pv = S.py[slot], pw = S.pz[slot];
 
+                // (x - x0) / h per axis: GetField's tap index and CurrentToMesh's
+                // start class both truncate it (divided once, the same bits)
+                const double ux = (x - x0) / hx, uy = (y - y0) / hy, uz = (z - z0) / hz;
+
                 // ---- Cell::GetField, cell.h:1257-1290 (InverseKernel 1010-1047)
                 double fEx, fEy, fEz, fHx, fHy, fHz;
                 if (x < 0 || y < 0 || z < 0) {
                     fEx = fEy = fEz = fHx = fHy = fHz = 0.0;
                 } else {
-                    int ix = (int)((x - x0) / hx + 1.0) + 1;
-                    int i1x = (int)(((x - x0) / hx + 1.0) + 1.5);
+                    int ix = (int)(ux + 1.0) + 1;
+                    int i1x = (int)((ux + 1.0) + 1.5);
                     double s1 = (int)(x / hx + 1.0) - x / hx;
                     double s2 = (int)(x / hx + 1.5) - 0.5 - x / hx;
-                    int iy = (int)((y - y0) / hy + 1.0) + 1;
-                    int i1y = (int)(((y - y0) / hy + 1.0) + 1.5);
+                    int iy = (int)(uy + 1.0) + 1;
+                    int i1y = (int)((uy + 1.0) + 1.5);
                     double s3 = (int)(y / hy + 1.0) - y / hy;
                     double s4 = (int)(y / hy + 1.5) - 0.5 - y / hy;
-                    int iz = (int)((z - z0) / hz + 1.0) + 1;
-                    int i1z = (int)(((z - z0) / hz + 1.0) + 1.5);
+                    int iz = (int)(uz + 1.0) + 1;
+                    int i1z = (int)((uz + 1.0) + 1.5);
                     double s5 = (int)(z / hz + 1.0) - z / hz;
                     double s6 = (int)(z / hz + 1.5) - 0.5 - z / hz;
                     double s11 = 1. - s1, s21 = 1. - s2, s31 = 1. - s3, s41 = 1. - s4, s51 = 1. - s5, s61 = 1. - s6;
@@ -438,22 +442,22 @@ __global__ void PIC_PLAIN_BOUNDS k_push_plain(StepParams P) {
                     pv = pv1 + fEy * tau1;
                     pw = pw1 + fEz * tau1;
                 }
-                ps = 1.0 / sqrt(((pu * pu + pv * pv + pw * pw) + 1.0));
+                // gamma = sqrt(p^2 + 1), for the new position and the kinetic energy
+                const double p2 = pu * pu + pv * pv + pw * pw;
+                const double gam = sqrt(p2 + 1.0);
+                ps = 1.0 / gam;
                 double xn[3] = {x + tau * (ps * pu), y + tau * (ps * pv), z + tau * (ps * pw)};
                 if (!(isfinite(pu) && isfinite(pv) && isfinite(pw))) bad |= ST_NAN;
-                {
-                    double p2 = pu * pu + pv * pv + pw * pw;
-                    kin += M * (p2 / (sqrt(1.0 + p2) + 1.0));  // gamma - 1 without cancellation
-                }
+                kin += M * (p2 / (gam + 1.0));  // gamma - 1 without cancellation
 
                 // ---- Cell::CurrentToMesh, cell.h:1306-1422
                 {
                     double xo[3] = {x, y, z}, x2[3] = {0.0, 0.0, 0.0}, sr;
-                    const double h3[3] = {hx, hy, hz}, o3[3] = {x0, y0, z0};
+                    const double h3[3] = {hx, hy, hz}, o3[3] = {x0, y0, z0}, r3[3] = {ux, uy, uz};
                     int i1[3], i2[3];
 #pragma unroll
                     for (int d = 0; d < 3; d++) {  // getCellNumberCenterCurrent, cell.h:577-578
-                        double tt = ((xo[d] - o3[d]) / h3[d] + 1.5);
+                        double tt = (r3[d] + 1.5);  // (xo - o3) / h3 + 1.5
                         i1[d] = (int)(tt + 1);
                         double t2 = ((xn[d] - o3[d]) / h3[d] + 1.5);
                         i2[d] = (int)(t2 + 1);
